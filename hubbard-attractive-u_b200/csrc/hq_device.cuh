@@ -1,0 +1,334 @@
+// hq_device.cuh -- device helpers of the sm_100a DQMC kernels:
+//   * the reference's random stream (std::default_random_engine = minstd_rand0 and
+//     std::bernoulli_distribution / generate_canonical<double,53> of libstdc++),
+//     replayed exactly with jump-ahead so every site of a slice gets its uniform at once;
+//   * FP64 tensor-core (DMMA, mma.sync m16n8k4 .f64) fragment helpers;
+//   * exp(-dt K) application: dense (DMMA) and separable (A (x) A circulant) forms;
+//   * block reductions.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "hq_types.h"
+
+namespace hq {
+
+// ------------------------------------------------------------------------------------
+//  minstd_rand0: x <- 16807 x mod (2^31 - 1)   (libstdc++ default_random_engine,
+//  src/random.cpp:14). generate_canonical<double, 53> draws two values:
+//     sum = (x1 - 1) + (x2 - 1) * R ;  ret = sum / round(R*R) ;  R = 2147483646
+//  with plain IEEE double operations (no contraction), clamped below 1.
+// ------------------------------------------------------------------------------------
+constexpr uint32_t kMinstdA = 16807u;
+constexpr uint32_t kMinstdM = 2147483647u;
+
+__host__ __device__ inline uint32_t minstd_mulmod(uint64_t a, uint64_t x) {
+  return static_cast<uint32_t>((a * x) % kMinstdM);
+}
+// a^k mod m
+__host__ __device__ inline uint32_t minstd_pow(uint64_t k) {
+  uint64_t result = 1, base = kMinstdA;
+  while (k) {
+    if (k & 1) result = (result * base) % kMinstdM;
+    base = (base * base) % kMinstdM;
+    k >>= 1;
+  }
+  return static_cast<uint32_t>(result);
+}
+
+__device__ inline double canonical_from_pair(uint32_t x1, uint32_t x2) {
+  const double R = 2147483646.0;
+  const double RR = __dmul_rn(R, R);
+  const double sum = __dadd_rn((double)(x1 - 1u), __dmul_rn((double)(x2 - 1u), R));
+  double r = __ddiv_rn(sum, RR);
+  if (r >= 1.0) r = 0.99999999999999988898;  // nextafter(1.0, 0.0)
+  return r;
+}
+
+// ------------------------------------------------------------------------------------
+//  DMMA m16n8k4 (FP64). Fragment ownership (lane = 4*g + q):
+//    A (16x4, row): a0 = A[g][q], a1 = A[g+8][q]
+//    B (4x8,  col): b0 = B[q][g]
+//    C (16x8)     : c0 = C[g][2q], c1 = C[g][2q+1], c2 = C[g+8][2q], c3 = C[g+8][2q+1]
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// ------------------------------------------------------------------------------------
+//  Reductions
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+// block-wide sum; red must hold >= 32 doubles; result valid in all threads
+__device__ inline double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = (lane < nw) ? red[lane] : 0.0;
+  t = warp_sum(t);
+  return t;
+}
+__device__ inline double block_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = (lane < nw) ? red[lane] : -INFINITY;
+  t = warp_max(t);
+  return t;
+}
+
+// atomic max on doubles (ordered-int trick; values may be negative)
+__device__ inline void atomic_max_double(double* addr, double val) {
+  unsigned long long* p = reinterpret_cast<unsigned long long*>(addr);
+  unsigned long long old = *p, assumed;
+  do {
+    assumed = old;
+    if (__longlong_as_double(assumed) >= val) return;
+    old = atomicCAS(p, assumed, __double_as_longlong(val));
+  } while (old != assumed);
+}
+
+// ------------------------------------------------------------------------------------
+//  Separable exp(-dt K): for the uniform NN hopping on the L x L torus,
+//    exp(-dt K) = exp(dt mu) * A (x) A,   A = exp(dt t H_1d) circulant, A[x][x'] = a[(x-x') mod L],
+//  with site index i = x + L y (src/square_lattice.cpp:30-61). Applied to a matrix M with
+//  leading dimension ld in two in-place passes of length-L circular convolutions.
+//  side 0: M <- c (A(x)A) M  (rows);  side 1: M <- c M (A(x)A)  (columns).
+//  rows/cols outside [0, N) are untouched. All threads of the block participate.
+// ------------------------------------------------------------------------------------
+template <int LT>
+__device__ inline void sep_pass(double* M, int ld, int N, int L, const double* __restrict__ a, double c, int side,
+                                int pass) {
+  // a fiber: fixed (other coordinate, matrix index); LT = compile-time bound on L
+  const int nfib = N * L;  // (N matrices-lines) x (L fibers per line)
+  for (int f = threadIdx.x; f < nfib; f += blockDim.x) {
+    const int line = f % N;   // column j (side 0) or row i (side 1)
+    const int o = f / N;      // the fixed coordinate of the fiber
+    double v[LT];
+    // element offset of fiber entry e (0 <= e < L)
+    // side 0 (rows, column `line`):  i = x + L y ; pass 0 runs over x with y = o, pass 1 over y with x = o
+    // side 1 (columns, row `line`):  j = x + L y ; same
+    const int base_site = (pass == 0) ? (L * o) : o;
+    const int step_site = (pass == 0) ? 1 : L;
+#pragma unroll
+    for (int e = 0; e < LT; ++e) {
+      if (e < L) {
+        const int s = base_site + e * step_site;
+        v[e] = (side == 0) ? M[s + (size_t)line * ld] : M[line + (size_t)s * ld];
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < LT; ++e) {
+      if (e < L) {
+        double acc = 0.0;
+#pragma unroll
+        for (int e2 = 0; e2 < LT; ++e2) {
+          if (e2 < L) {
+            int d = e - e2;
+            d += (d < 0) ? L : 0;
+            acc = fma(a[d], v[e2], acc);
+          }
+        }
+        if (pass == 1) acc *= c;
+        const int s = base_site + e * step_site;
+        if (side == 0) M[s + (size_t)line * ld] = acc; else M[line + (size_t)s * ld] = acc;
+      }
+    }
+  }
+}
+
+template <int LT>
+__device__ inline void sep_apply(double* M, int ld, int N, int L, const double* a, double c, int side) {
+  sep_pass<LT>(M, ld, N, L, a, c, side, 0);
+  __syncthreads();
+  sep_pass<LT>(M, ld, N, L, a, c, side, 1);
+  __syncthreads();
+}
+
+// dispatch on L to a compile-time fiber length
+__device__ inline void sep_apply_any(double* M, int ld, int N, int L, const double* a, double c, int side) {
+  if (L <= 4) sep_apply<4>(M, ld, N, L, a, c, side);
+  else if (L <= 8) sep_apply<8>(M, ld, N, L, a, c, side);
+  else if (L <= 12) sep_apply<12>(M, ld, N, L, a, c, side);
+  else sep_apply<16>(M, ld, N, L, a, c, side);
+}
+
+// ------------------------------------------------------------------------------------
+//  Dense exp(-dt K) application with DMMA, M in shared (or global) memory, E in global
+//  (L2-resident: shared by every chain of the same parameters).
+//  dense_apply:       M <- E M, by column blocks (E M[:, blk] needs only blk)
+//  dense_apply_right: M <- M E, by row blocks    (M[blk, :] E needs only blk)
+//  E is symmetric here (K real symmetric), so op(E) = E in both cases.
+//  stage: shared scratch of >= 2 * (N16 * 8) doubles used to stage k-chunks of E.
+//  The output of a block is accumulated in registers (<= kMaxFrag fragments per warp).
+// ------------------------------------------------------------------------------------
+constexpr int kMaxFrag = 8;
+
+__device__ inline void dense_apply(double* M, int ld, int N, const double* __restrict__ E, double* stage) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int N16 = (N + 15) & ~15;       // padded row count
+  const int mt = N16 / 16;              // 16-row tiles
+  const int max_tiles = kMaxFrag * nwarps;
+  int cb8 = max_tiles / mt;             // 8-wide column tiles per block
+  if (cb8 < 1) cb8 = 1;
+  const int nt8 = (N + 7) / 8;
+  if (cb8 > nt8) cb8 = nt8;
+  const int CB = cb8 * 8;
+  const int lds = N16 + 4;              // stage leading dimension
+  for (int c0 = 0; c0 < N; c0 += CB) {
+    const int tiles = mt * cb8;
+    double acc[kMaxFrag][4];
+#pragma unroll
+    for (int f = 0; f < kMaxFrag; ++f) acc[f][0] = acc[f][1] = acc[f][2] = acc[f][3] = 0.0;
+    for (int k0 = 0; k0 < N; k0 += 8) {
+      // stage[kk * lds + r] = E[r, k0 + kk]
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < 8 * N16; idx += blockDim.x) {
+        const int kk = idx / N16, r = idx % N16;
+        const int k = k0 + kk;
+        stage[kk * lds + r] = (r < N && k < N) ? E[r + (size_t)k * N] : 0.0;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int f = 0; f < kMaxFrag; ++f) {
+        const int tile = warp + f * nwarps;
+        if (tile < tiles) {
+          const int tm = tile % mt, tn = tile / mt;
+          const int r = tm * 16 + g;
+          const int cc = c0 + tn * 8 + g;
+#pragma unroll
+          for (int ks = 0; ks < 8; ks += 4) {
+            const int k = k0 + ks + q;
+            const double a0 = stage[(ks + q) * lds + r];
+            const double a1 = stage[(ks + q) * lds + r + 8];
+            const double b0 = (k < N && cc < N) ? M[k + (size_t)cc * ld] : 0.0;
+            dmma_16x8x4(acc[f], a0, a1, b0);
+          }
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int f = 0; f < kMaxFrag; ++f) {
+      const int tile = warp + f * nwarps;
+      if (tile < tiles) {
+        const int tm = tile % mt, tn = tile / mt;
+        const int r = tm * 16 + g, c = c0 + tn * 8 + 2 * q;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int rr = r + ((e & 2) ? 8 : 0), cc = c + (e & 1);
+          if (rr < N && cc < N && cc < c0 + CB) M[rr + (size_t)cc * ld] = acc[f][e];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// side-1 dense application uses row blocks of height CB where the tiles enumerate
+// (8-col tiles over all N) x (16-row tiles inside the block); keep the block height a
+// multiple of 16 and the tile count within kMaxFrag * nwarps.
+__device__ inline void dense_apply_right(double* M, int ld, int N, const double* __restrict__ E, double* stage) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int N8 = (N + 7) & ~7;
+  const int nt8 = N8 / 8;                // 8-col tiles over all columns
+  const int max_tiles = kMaxFrag * nwarps;
+  int rb16 = max_tiles / nt8;            // 16-row tiles per block
+  if (rb16 < 1) rb16 = 1;
+  const int mt16 = (N + 15) / 16;
+  if (rb16 > mt16) rb16 = mt16;
+  const int RB = rb16 * 16;
+  const int lds = N8 + 4;
+  for (int r0 = 0; r0 < N; r0 += RB) {
+    const int tiles = nt8 * rb16;
+    double acc[kMaxFrag][4];
+#pragma unroll
+    for (int f = 0; f < kMaxFrag; ++f) acc[f][0] = acc[f][1] = acc[f][2] = acc[f][3] = 0.0;
+    for (int k0 = 0; k0 < N; k0 += 8) {
+      __syncthreads();
+      // stage[kk * lds + c] = E[k0+kk, c]
+      for (int idx = threadIdx.x; idx < 8 * N8; idx += blockDim.x) {
+        const int kk = idx / N8, c = idx % N8;
+        const int k = k0 + kk;
+        stage[kk * lds + c] = (c < N && k < N) ? E[k + (size_t)c * N] : 0.0;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int f = 0; f < kMaxFrag; ++f) {
+        const int tile = warp + f * nwarps;
+        if (tile < tiles) {
+          const int tc = tile % nt8, tr = tile / nt8;
+#pragma unroll
+          for (int ks = 0; ks < 8; ks += 4) {
+            const int k = k0 + ks + q;
+            const int r = r0 + tr * 16 + g;
+            const double a0 = (r < N && k < N) ? M[r + (size_t)k * ld] : 0.0;
+            const double a1 = (r + 8 < N && k < N) ? M[r + 8 + (size_t)k * ld] : 0.0;
+            const double b0 = stage[(ks + q) * lds + tc * 8 + g];
+            dmma_16x8x4(acc[f], a0, a1, b0);
+          }
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int f = 0; f < kMaxFrag; ++f) {
+      const int tile = warp + f * nwarps;
+      if (tile < tiles) {
+        const int tc = tile % nt8, tr = tile / nt8;
+        const int r = r0 + tr * 16 + g, c = tc * 8 + 2 * q;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int rr = r + ((e & 2) ? 8 : 0), cc = c + (e & 1);
+          if (rr < N && cc < N && rr < r0 + RB) M[rr + (size_t)cc * ld] = acc[f][e];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// M <- diag(v) M (rows) with v_i = (s_i > 0 ? vp : vm) ; fields is the slice's int8 row
+__device__ inline void scale_rows(double* M, int ld, int N, const int8_t* s, double vp, double vm) {
+  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+    const int i = idx % N, j = idx / N;
+    M[i + (size_t)j * ld] *= (s[i] > 0 ? vp : vm);
+  }
+}
+// M <- M diag(v) (columns)
+__device__ inline void scale_cols(double* M, int ld, int N, const int8_t* s, double vp, double vm) {
+  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+    const int i = idx % N, j = idx / N;
+    M[i + (size_t)j * ld] *= (s[j] > 0 ? vp : vm);
+  }
+}
+
+// M <- expK M   (side 0)  /  M <- M expK (side 1); inv selects inv_expK
+__device__ inline void apply_expk(const HqChain& ch, double* M, int ld, int side, bool inv, double* stage) {
+  if (ch.expk_mode == HQK_EXPK_SEPARABLE) {
+    sep_apply_any(M, ld, ch.N, ch.L, inv ? ch.sep_ai : ch.sep_a, inv ? ch.sep_ci : ch.sep_c, side);
+  } else {
+    const double* E = inv ? ch.inv_expK : ch.expK;
+    if (side == 0) dense_apply(M, ld, ch.N, E, stage);
+    else dense_apply_right(M, ld, ch.N, E, stage);
+  }
+}
+
+}  // namespace hq

@@ -1,0 +1,1118 @@
+// hq_kernels.cu -- sm_100a kernels of the batched DQMC sweep (FP64).
+//
+//  k_interval  : one CTA per chain, G(tau,tau) resident in shared memory for a whole
+//                stabilisation interval: wrap (src/dqmc_core.cpp:142-161), Metropolis
+//                flips with delayed rank-k updates flushed by DMMA
+//                (src/dqmc_core.cpp:102-119, src/hubbard.cpp:123-139), fused equal-time
+//                estimators (include/observable_methods.hpp:39-151) and optional snapshots.
+//  k_bchain    : B-matrix chain of one interval applied to U_top*D_top
+//                (src/dqmc_core.cpp:190, :251 + the (M*U)*S product of svd_stack.hpp:144).
+//  k_udt       : column-pivoted Householder UDV factorisation X P = Q R, X = Q D T
+//                (the stack push of include/utils/svd_stack.hpp:107-175).
+//  k_invert    : in-place Gauss-Jordan inverse with partial pivoting (the inverse() of
+//                include/utils/stable_numerics.hpp:235).
+//  k_gemm      : batched FP64 DMMA GEMM with the scalings of the G builders
+//                (include/utils/stable_numerics.hpp:186-324) and the wrap-error epilogue
+//                (:37-48, signed maximum).
+//  k_measure   : equal-time estimators + snapshot of a freshly built G.
+//  k_dyn_*     : time-displaced propagation and estimators (src/dqmc_core.cpp:291-390,
+//                include/observable_methods.hpp:84-195).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <climits>
+#include "hq_device.cuh"
+#include "hq_kernels.h"
+
+namespace hq {
+
+// shared-memory leading dimension of an N x N matrix: odd, so that threads walking
+// consecutive columns hit distinct banks
+__host__ __device__ inline int smem_ld(int N) { return (N % 2 == 0) ? N + 1 : N; }
+
+// bytes of dynamic shared memory of k_interval / k_bchain for a chain of size N with
+// delay depth kmax (matrix in smem when `resident`)
+__host__ __device__ inline size_t interval_smem_doubles(int N, int kmax, bool resident) {
+  const size_t mat = resident ? (size_t)N * smem_ld(N) : 0;
+  const size_t panels = (size_t)N * kmax * 2;
+  const size_t stage = (size_t)8 * (((N + 15) & ~15) + 4);
+  const size_t work = panels > stage ? panels : stage;
+  return mat + work + 3 * (size_t)N + (size_t)(N + 7) / 4 + 64;
+}
+
+struct SliceView {
+  const int8_t* s;  // fields of the slice (shared memory)
+};
+
+// ---------------------------------------------------------------------------------
+//  Equal-time estimators of one slice (include/observable_methods.hpp:39-74, 131-151)
+//  filling = 2 - 2 trG/N ; docc = sum_i (1-G_ii)^2 / N ;
+//  swave   = sum_ij [(1-G)_ji^2 + G_ij^2] / N = (2 sum G^2 - 2 trG + N) / N
+// ---------------------------------------------------------------------------------
+__device__ void measure_slice(const double* G, int ld, int N, double* acc, double* red) {
+  double tr = 0.0, dd = 0.0, sq = 0.0;
+  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+    const int i = idx % N, j = idx / N;
+    const double v = G[i + (size_t)j * ld];
+    sq += v * v;
+    if (i == j) { tr += v; dd += (1.0 - v) * (1.0 - v); }
+  }
+  tr = block_sum(tr, red);
+  dd = block_sum(dd, red);
+  sq = block_sum(sq, red);
+  if (threadIdx.x == 0) {
+    acc[HQ_ACC_FILLING] += 2.0 - 2.0 * tr / N;
+    acc[HQ_ACC_DOCC] += dd / N;
+    acc[HQ_ACC_SWAVE] += (2.0 * sq - 2.0 * tr + N) / N;
+    acc[HQ_ACC_NSLICE] += 1.0;
+  }
+}
+
+__device__ void copy_mat(double* dst, int ldd, const double* src, int lds, int N) {
+  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+    const int i = idx % N, j = idx / N;
+    dst[i + (size_t)j * ldd] = src[i + (size_t)j * lds];
+  }
+}
+
+// ---------------------------------------------------------------------------------
+//  Metropolis sweep over the N sites of one slice with delayed rank-k updates.
+//
+//  The reference visits i = 0..N-1 in order, draws one uniform per site, and on
+//  acceptance applies G -= gamma G[:,i] (e_i^T - G[i,:]), gamma = Delta/(1+(1-G_ii)Delta)
+//  (src/hubbard.cpp:123-139). A rejected site leaves G unchanged, so the ratio of every
+//  later site only depends on the current diagonal: all remaining sites are tested in
+//  parallel and the first acceptance is taken, then the search resumes after it. The
+//  accepted updates are kept as G = G0 + X Y (X: N x k, Y: k x N) and flushed into G0
+//  with DMMA when k reaches kmax and at the end of the slice.
+// ---------------------------------------------------------------------------------
+__device__ void flush_panels(double* G, int ld, int N, const double* X, int ldx, const double* Y, int ldy, int k) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int mt = (N + 15) / 16, nt8 = (N + 7) / 8;
+  const int tiles = mt * nt8;
+  for (int tile = warp; tile < tiles; tile += nwarps) {
+    const int r0 = (tile % mt) * 16, c0 = (tile / mt) * 8;
+    const int r = r0 + g, c = c0 + 2 * q;
+    double acc[4];
+    acc[0] = (r < N && c < N) ? G[r + (size_t)c * ld] : 0.0;
+    acc[1] = (r < N && c + 1 < N) ? G[r + (size_t)(c + 1) * ld] : 0.0;
+    acc[2] = (r + 8 < N && c < N) ? G[r + 8 + (size_t)c * ld] : 0.0;
+    acc[3] = (r + 8 < N && c + 1 < N) ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
+    for (int m0 = 0; m0 < k; m0 += 4) {
+      const int m = m0 + q;
+      const double a0 = (r < N && m < k) ? X[r + m * ldx] : 0.0;
+      const double a1 = (r + 8 < N && m < k) ? X[r + 8 + m * ldx] : 0.0;
+      const int cb = c0 + g;
+      const double b0 = (cb < N && m < k) ? Y[m * ldy + cb] : 0.0;
+      dmma_16x8x4(acc, a0, a1, b0);
+    }
+    if (r < N && c < N) G[r + (size_t)c * ld] = acc[0];
+    if (r < N && c + 1 < N) G[r + (size_t)(c + 1) * ld] = acc[1];
+    if (r + 8 < N && c < N) G[r + 8 + (size_t)c * ld] = acc[2];
+    if (r + 8 < N && c + 1 < N) G[r + 8 + (size_t)(c + 1) * ld] = acc[3];
+  }
+}
+
+struct MetroShared {
+  double* d;      // current diagonal [N]
+  double* u;      // uniforms [N]
+  double* rr;     // last ratio of each site [N] (ratio log)
+  int8_t* s;      // fields of the slice [N]
+  int8_t* flip;   // accepted flags [N]
+  double* X;      // N x kmax
+  double* Y;      // kmax x N (row-major)
+  int* ired;      // >= 32 ints
+};
+
+__device__ void metropolis_slice(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
+                                 double& n_acc, int flags, long long log_base) {
+  const int N = ch.N, kmax = ch.kmax;
+  const int ldx = N, ldy = N;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  // uniforms of this slice: site i consumes engine draws 2i+1, 2i+2 after the current state
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const uint32_t x1 = minstd_mulmod(minstd_pow(2ull * i + 1), rng);
+    const uint32_t x2 = minstd_mulmod(kMinstdA, x1);
+    sh.u[i] = canonical_from_pair(x1, x2);
+    sh.d[i] = G[i + (size_t)i * ld];
+    sh.flip[i] = 0;
+  }
+  rng = minstd_mulmod(minstd_pow(2ull * N), rng);
+  __syncthreads();
+  int k = 0, start = 0;
+  while (true) {
+    // ---- find the first accepted site in [start, N) ----
+    int cand = INT_MAX;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      if (i >= start) {
+        const double delta = sh.s[i] > 0 ? ch.delta_p : ch.delta_m;
+        const double a = 1.0 + (1.0 - sh.d[i]) * delta;
+        const double r = (a * a) / (1.0 + delta);
+        sh.rr[i] = r;
+        if (sh.u[i] < fmin(1.0, fabs(r)) && i < cand) cand = i;
+      }
+    }
+    cand = __reduce_min_sync(0xffffffffu, cand);
+    if (lane == 0) sh.ired[warp] = cand;
+    __syncthreads();
+    int first = INT_MAX;
+    for (int w = 0; w < nwarps; ++w) first = min(first, sh.ired[w]);
+    if (first == INT_MAX) break;
+    // ---- accept site j: append gamma*G[:,j] and (G[j,:] - e_j) to the panels ----
+    const int j = first;
+    const double delta = sh.s[j] > 0 ? ch.delta_p : ch.delta_m;
+    const double gamma = delta / (1.0 + (1.0 - sh.d[j]) * delta);
+    for (int p = threadIdx.x; p < N; p += blockDim.x) {
+      double col = G[p + (size_t)j * ld];
+      double row = G[j + (size_t)p * ld];
+      for (int m = 0; m < k; ++m) {
+        col = fma(sh.X[p + m * ldx], sh.Y[m * ldy + j], col);
+        row = fma(sh.X[j + m * ldx], sh.Y[m * ldy + p], row);
+      }
+      const double xv = gamma * col;
+      const double yv = row - (p == j ? 1.0 : 0.0);
+      sh.X[p + k * ldx] = xv;
+      sh.Y[k * ldy + p] = yv;
+      if (p != j) sh.d[p] = fma(xv, yv, sh.d[p]);
+      else sh.flip[p] = 1;
+    }
+    n_acc += 1.0;
+    ++k;
+    start = j + 1;
+    __syncthreads();
+    if (k == kmax) {
+      flush_panels(G, ld, N, sh.X, ldx, sh.Y, ldy, k);
+      k = 0;
+      __syncthreads();
+    }
+  }
+  if (k > 0) {
+    flush_panels(G, ld, N, sh.X, ldx, sh.Y, ldy, k);
+  }
+  // apply the flips of this slice and optionally log the visit-time ratios
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    if (sh.flip[i]) sh.s[i] = -sh.s[i];
+    if ((flags & HQ_F_LOG_RATIOS) && ch.ratios && log_base + i < ch.ratio_cap) ch.ratios[log_base + i] = sh.rr[i];
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------
+//  wrap of G by B(l) (src/dqmc_core.cpp:142-161, src/hubbard.cpp:293-331)
+//   up  : G <- e^{V_l} E G E^{-1} e^{-V_l}
+//   down: G <- E^{-1} e^{-V_l} G e^{V_l} E
+// ---------------------------------------------------------------------------------
+__device__ void wrap_slice(const HqChain& ch, double* G, int ld, const int8_t* s, int dir, double* stage) {
+  const int N = ch.N;
+  if (dir == HQ_UP) {
+    apply_expk(ch, G, ld, 0, false, stage);
+    apply_expk(ch, G, ld, 1, true, stage);
+    for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+      const int i = idx % N, j = idx / N;
+      const double fi = s[i] > 0 ? ch.ev_p : ch.ev_m;
+      const double fj = s[j] > 0 ? ch.ev_m : ch.ev_p;
+      G[i + (size_t)j * ld] *= fi * fj;
+    }
+    __syncthreads();
+  } else {
+    for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+      const int i = idx % N, j = idx / N;
+      const double fi = s[i] > 0 ? ch.ev_m : ch.ev_p;
+      const double fj = s[j] > 0 ? ch.ev_p : ch.ev_m;
+      G[i + (size_t)j * ld] *= fi * fj;
+    }
+    __syncthreads();
+    apply_expk(ch, G, ld, 0, true, stage);
+    apply_expk(ch, G, ld, 1, false, stage);
+  }
+}
+
+// slice range of interval b: up-sweep intervals are [b*pace+1, min((b+1)*pace, nt)];
+// the down sweep visits the same intervals from the top (b counts from tau = beta)
+__device__ __host__ inline void interval_range(int nt, int pace, int n_stab, int dir, int b, int& t_lo, int& t_hi) {
+  const int bu = (dir == HQ_DOWN) ? (n_stab - 1 - b) : b;
+  t_lo = bu * pace + 1;
+  t_hi = min((bu + 1) * pace, nt);
+}
+
+// ---------------------------------------------------------------------------------
+//  k_interval: the update (or no-update) slices of one stabilisation interval.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(HQ_THREADS, 1)
+k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int flags, int resident) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ HqChain ch;
+  __shared__ double red[32];
+  __shared__ int ired[32];
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  if (threadIdx.x == 0) ch = chains[c];
+  __syncthreads();
+  if (!ch.active || b >= ch.n_stab) return;
+  const int N = ch.N;
+  int t_lo, t_hi;
+  interval_range(ch.nt, ch.pace, ch.n_stab, dir, b, t_lo, t_hi);
+
+  // shared-memory carve-up
+  double* p = smem;
+  double* G;
+  int ld;
+  if (resident) {
+    G = p;
+    ld = smem_ld(N);
+    p += (size_t)N * ld;
+    copy_mat(G, ld, ch.G, N, N);
+  } else {
+    G = ch.G;
+    ld = N;
+  }
+  const size_t panels = (size_t)N * ch.kmax * 2;
+  const size_t stage_n = (size_t)8 * (((N + 15) & ~15) + 4);
+  double* work = p;
+  p += panels > stage_n ? panels : stage_n;
+  MetroShared sh;
+  sh.X = work;
+  sh.Y = work + (size_t)N * ch.kmax;
+  sh.d = p; p += N;
+  sh.u = p; p += N;
+  sh.rr = p; p += N;
+  sh.s = reinterpret_cast<int8_t*>(p);
+  sh.flip = sh.s + N;
+  sh.ired = ired;
+  uint32_t rng = *ch.rng;
+  double n_acc = 0.0, n_prop = 0.0;
+  long long log_base = (flags & HQ_F_LOG_RATIOS) && ch.ratio_count ? *ch.ratio_count : 0;
+  __syncthreads();
+
+  const int nsl = t_hi - t_lo + 1;
+  for (int step = 0; step < nsl; ++step) {
+    const int t = (dir == HQ_DOWN) ? (t_hi - step) : (t_lo + step);
+    const int l = t % ch.nt;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) sh.s[i] = ch.fields[(size_t)l * N + i];
+    __syncthreads();
+    if (dir == HQ_UP) {
+      wrap_slice(ch, G, ld, sh.s, HQ_UP, work);
+      metropolis_slice(ch, G, ld, sh, rng, n_acc, flags, log_base);
+      n_prop += N;
+      log_base += N;
+    } else if (dir == HQ_DOWN) {
+      metropolis_slice(ch, G, ld, sh, rng, n_acc, flags, log_base);
+      n_prop += N;
+      log_base += N;
+      wrap_slice(ch, G, ld, sh.s, HQ_DOWN, work);
+    } else {
+      wrap_slice(ch, G, ld, sh.s, HQ_UP, work);
+    }
+    for (int i = threadIdx.x; i < N; i += blockDim.x) ch.fields[(size_t)l * N + i] = sh.s[i];
+    // the last slice of the interval is measured after stabilisation
+    if (step < nsl - 1) {
+      const int lm = (dir == HQ_DOWN) ? ((t - 1) % ch.nt) : l;
+      if (flags & HQ_F_MEASURE) measure_slice(G, ld, N, ch.acc, red);
+      if ((flags & HQ_F_SNAPSHOT) && ch.snap_tt) copy_mat(ch.snap_tt + (size_t)lm * N * N, N, G, ld, N);
+    }
+    __syncthreads();
+  }
+  if (resident) copy_mat(ch.G, N, G, ld, N);
+  if (threadIdx.x == 0) {
+    *ch.rng = rng;
+    ch.acc[HQ_ACC_PROPOSED] += n_prop;
+    ch.acc[HQ_ACC_ACCEPTED] += n_acc;
+    if ((flags & HQ_F_LOG_RATIOS) && ch.ratio_count) *ch.ratio_count = log_base;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+//  k_bchain: X <- (U_top diag(D_top) or 1), then the B products of interval b:
+//   up  : X <- B(t) X = e^{V_t} E X, t ascending            (src/dqmc_core.cpp:190)
+//   down: X <- B(t)^T X = E e^{V_t} X, t descending           (src/dqmc_core.cpp:251)
+//  dir UP pushes onto the left stack, DOWN onto the right stack; that stack holds b
+//  entries before the push (top entry b-1, none when b = 0).
+//  init: the right stack at initialisation (src/dqmc_core.cpp:67-87) is the down
+//  direction without updates.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(HQ_THREADS, 1)
+k_bchain(const HqChain* __restrict__ chains, int nchains, int dir, int b, int resident) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ HqChain ch;
+  __shared__ int8_t s[HQ_MAX_N];
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  if (threadIdx.x == 0) ch = chains[c];
+  __syncthreads();
+  if (!ch.active || b >= ch.n_stab) return;
+  const int N = ch.N;
+  int t_lo, t_hi;
+  interval_range(ch.nt, ch.pace, ch.n_stab, dir, b, t_lo, t_hi);
+  const int side = (dir == HQ_DOWN) ? 1 : 0;
+  const int top = b - 1;  // the pushing stack holds b entries before this push
+  double* X;
+  int ld;
+  double* p = smem;
+  if (resident) { X = p; ld = smem_ld(N); p += (size_t)N * ld; } else { X = ch.X; ld = N; }
+  double* stage = p;
+  const size_t NN = (size_t)N * N;
+  const double* U = top >= 0 ? ch.stackU + ((size_t)side * ch.n_stab + top) * NN : nullptr;
+  const double* D = top >= 0 ? ch.stackD + ((size_t)side * ch.n_stab + top) * N : nullptr;
+  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+    const int i = idx % N, j = idx / N;
+    X[i + (size_t)j * ld] = U ? U[idx] * D[j] : (i == j ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  const int nsl = t_hi - t_lo + 1;
+  for (int step = 0; step < nsl; ++step) {
+    const int t = (dir == HQ_DOWN) ? (t_hi - step) : (t_lo + step);
+    const int l = t % ch.nt;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s[i] = ch.fields[(size_t)l * N + i];
+    __syncthreads();
+    if (dir == HQ_DOWN) {
+      scale_rows(X, ld, N, s, ch.ev_p, ch.ev_m);
+      __syncthreads();
+      apply_expk(ch, X, ld, 0, false, stage);
+    } else {
+      apply_expk(ch, X, ld, 0, false, stage);
+      scale_rows(X, ld, N, s, ch.ev_p, ch.ev_m);
+      __syncthreads();
+    }
+  }
+  if (resident) copy_mat(ch.X, N, X, ld, N);
+}
+
+// ---------------------------------------------------------------------------------
+//  k_udt: X P = Q R (column-pivoted Householder QR, LAPACK dgeqp3/dlaqp2 order), then
+//  D = |diag R|, T = D^-1 R P^T, and Q formed in place (dorg2r order).
+//  Output: U -> stack entry, D -> stack entry, T -> W0.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(HQ_THREADS, 1)
+k_udt(const HqChain* __restrict__ chains, int nchains, int side, int entry_from_len, int b, int resident) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ HqChain ch;
+  __shared__ double red[32];
+  __shared__ int piv_s;
+  __shared__ double tau_s, beta_s;
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  if (threadIdx.x == 0) ch = chains[c];
+  __syncthreads();
+  if (!ch.active || b >= ch.n_stab) return;
+  const int N = ch.N;
+  const int entry = b;  // push position: the pushing stack holds b entries
+  double* A;
+  int ld;
+  double* p = smem;
+  if (resident) { A = p; ld = smem_ld(N); p += (size_t)N * ld; copy_mat(A, ld, ch.X, N, N); }
+  else { A = ch.X; ld = N; }
+  double* vn1 = p; p += N;
+  double* vn2 = p; p += N;
+  double* tau = p; p += N;
+  double* wv = p; p += N;
+  int* jpvt = reinterpret_cast<int*>(p);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  __syncthreads();
+  // column norms
+  for (int j = warp; j < N; j += nwarps) {
+    double s2 = 0.0;
+    for (int i = lane; i < N; i += 32) { const double v = A[i + (size_t)j * ld]; s2 = fma(v, v, s2); }
+    s2 = warp_sum(s2);
+    if (lane == 0) { vn1[j] = sqrt(s2); vn2[j] = vn1[j]; jpvt[j] = j; }
+  }
+  __syncthreads();
+  const double tol3z = sqrt(2.220446049250313e-16);
+  for (int i = 0; i < N; ++i) {
+    // pivot: argmax vn1[i:N] (first maximum, as idamax)
+    if (warp == 0) {
+      double best = -1.0;
+      int bi = i;
+      for (int j = i + lane; j < N; j += 32) {
+        const double v = vn1[j];
+        if (v > best) { best = v; bi = j; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (lane == 0) piv_s = bi;
+    }
+    __syncthreads();
+    const int pv = piv_s;
+    if (pv != i) {
+      for (int r = threadIdx.x; r < N; r += blockDim.x) {
+        const double t0 = A[r + (size_t)pv * ld];
+        A[r + (size_t)pv * ld] = A[r + (size_t)i * ld];
+        A[r + (size_t)i * ld] = t0;
+      }
+      if (threadIdx.x == 0) {
+        const int tj = jpvt[pv]; jpvt[pv] = jpvt[i]; jpvt[i] = tj;
+        vn1[pv] = vn1[i];
+        vn2[pv] = vn2[i];
+      }
+    }
+    __syncthreads();
+    // Householder reflector of A[i:N, i] (dlarfg)
+    double xs = 0.0;
+    for (int r = i + 1 + threadIdx.x; r < N; r += blockDim.x) { const double v = A[r + (size_t)i * ld]; xs = fma(v, v, xs); }
+    xs = block_sum(xs, red);
+    if (threadIdx.x == 0) {
+      const double alpha = A[i + (size_t)i * ld];
+      const double xnorm = sqrt(xs);
+      if (xnorm == 0.0) { tau_s = 0.0; beta_s = alpha; }
+      else {
+        const double beta = -copysign(hypot(alpha, xnorm), alpha);
+        tau_s = (beta - alpha) / beta;
+        beta_s = beta;
+        wv[0] = 1.0 / (alpha - beta);
+      }
+    }
+    __syncthreads();
+    const double ti = tau_s;
+    if (ti != 0.0) {
+      const double sc = wv[0];
+      for (int r = i + 1 + threadIdx.x; r < N; r += blockDim.x) A[r + (size_t)i * ld] *= sc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) { A[i + (size_t)i * ld] = beta_s; tau[i] = ti; }
+    // apply H = I - tau v v^T to A[i:N, i+1:N], v = [1; A[i+1:N, i]]; one warp per column
+    if (ti != 0.0) {
+      for (int j = i + 1 + warp; j < N; j += nwarps) {
+        double w = (lane == 0) ? A[i + (size_t)j * ld] : 0.0;
+        for (int r = i + 1 + lane; r < N; r += 32) w = fma(A[r + (size_t)i * ld], A[r + (size_t)j * ld], w);
+        w = warp_sum(w) * ti;
+        if (lane == 0) A[i + (size_t)j * ld] -= w;
+        for (int r = i + 1 + lane; r < N; r += 32) A[r + (size_t)j * ld] = fma(-w, A[r + (size_t)i * ld], A[r + (size_t)j * ld]);
+      }
+    }
+    __syncthreads();
+    // partial column norm downdate (dlaqp2)
+    for (int j = i + 1 + warp; j < N; j += nwarps) {
+      double nv1 = vn1[j];
+      if (nv1 != 0.0) {
+        double temp = fabs(A[i + (size_t)j * ld]) / nv1;
+        temp = 1.0 - temp * temp;
+        temp = fmax(temp, 0.0);
+        const double r2 = nv1 / vn2[j];
+        const double temp2 = temp * r2 * r2;
+        if (temp2 <= tol3z) {
+          double s2 = 0.0;
+          for (int r = i + 1 + lane; r < N; r += 32) { const double v = A[r + (size_t)j * ld]; s2 = fma(v, v, s2); }
+          s2 = warp_sum(s2);
+          if (lane == 0) { vn1[j] = sqrt(s2); vn2[j] = vn1[j]; }
+        } else {
+          if (lane == 0) vn1[j] = nv1 * sqrt(temp);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // D and T = D^-1 R P^T (T[:, jpvt[c]] = row-scaled R[:, c])
+  const size_t NN = (size_t)N * N;
+  double* Dout = ch.stackD + ((size_t)side * ch.n_stab + entry) * N;
+  double* T = ch.W0;
+  for (int r = threadIdx.x; r < N; r += blockDim.x) {
+    const double dr = fabs(A[r + (size_t)r * ld]);
+    Dout[r] = dr;
+    wv[r] = dr;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+    const int r = idx % N, cc = idx / N;
+    const double v = (r <= cc) ? A[r + (size_t)cc * ld] / wv[r] : 0.0;
+    T[r + (size_t)jpvt[cc] * N] = (wv[r] != 0.0) ? v : (r == cc ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  // form Q in place from the reflectors (dorg2r): for i = N-1 .. 0
+  for (int i = N - 1; i >= 0; --i) {
+    const double ti = tau[i];
+    if (i < N - 1) {
+      if (threadIdx.x == 0) A[i + (size_t)i * ld] = 1.0;
+      __syncthreads();
+      // apply H(i) to A[i:N, i+1:N]
+      for (int j = i + 1 + warp; j < N; j += nwarps) {
+        double w = 0.0;
+        for (int r = i + lane; r < N; r += 32) w = fma(A[r + (size_t)i * ld], A[r + (size_t)j * ld], w);
+        w = warp_sum(w) * ti;
+        for (int r = i + lane; r < N; r += 32) A[r + (size_t)j * ld] = fma(-w, A[r + (size_t)i * ld], A[r + (size_t)j * ld]);
+      }
+      __syncthreads();
+      for (int r = i + 1 + threadIdx.x; r < N; r += blockDim.x) A[r + (size_t)i * ld] *= -ti;
+    }
+    if (threadIdx.x == 0) A[i + (size_t)i * ld] = 1.0 - ti;
+    for (int r = threadIdx.x; r < i; r += blockDim.x) A[r + (size_t)i * ld] = 0.0;
+    __syncthreads();
+  }
+  double* Uout = ch.stackU + ((size_t)side * ch.n_stab + entry) * NN;
+  copy_mat(Uout, N, A, ld, N);
+}
+
+// ---------------------------------------------------------------------------------
+//  k_invert: in-place Gauss-Jordan inverse with partial (row) pivoting of the N x N
+//  matrix at `which` (0: W1, 1: W2, 2: W3, 3: W5). Failure (zero pivot / non-finite) sets acc[STATUS].
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(HQ_THREADS, 1)
+k_invert(const HqChain* __restrict__ chains, int nchains, int b, int which, int resident) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ HqChain ch;
+  __shared__ int piv_s;
+  __shared__ double pinv_s;
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  if (threadIdx.x == 0) ch = chains[c];
+  __syncthreads();
+  if (!ch.active || b >= ch.n_stab) return;
+  const int N = ch.N;
+  double* src = which == 0 ? ch.W1 : (which == 1 ? ch.W2 : (which == 2 ? ch.W3 : ch.W5));
+  double* A;
+  int ld;
+  double* p = smem;
+  if (resident) { A = p; ld = smem_ld(N); p += (size_t)N * ld; copy_mat(A, ld, src, N, N); }
+  else { A = src; ld = N; }
+  double* colk = p; p += N;
+  int* perm = reinterpret_cast<int*>(p);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  for (int k = 0; k < N; ++k) {
+    if (warp == 0) {
+      double best = -1.0;
+      int bi = k;
+      for (int r = k + lane; r < N; r += 32) {
+        const double v = fabs(A[r + (size_t)k * ld]);
+        if (v > best) { best = v; bi = r; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (lane == 0) {
+        piv_s = bi;
+        perm[k] = bi;
+        if (!(best > 0.0) || !isfinite(best)) ch.acc[HQ_ACC_STATUS] = 1.0;
+      }
+    }
+    __syncthreads();
+    const int pr = piv_s;
+    if (pr != k) {
+      for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        const double t0 = A[k + (size_t)j * ld];
+        A[k + (size_t)j * ld] = A[pr + (size_t)j * ld];
+        A[pr + (size_t)j * ld] = t0;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const double pv = A[k + (size_t)k * ld];
+      pinv_s = (pv != 0.0) ? 1.0 / pv : 0.0;
+    }
+    __syncthreads();
+    const double pinv = pinv_s;
+    // save column k, scale pivot row, with A[k,k] := 1 before scaling
+    for (int r = threadIdx.x; r < N; r += blockDim.x) colk[r] = A[r + (size_t)k * ld];
+    __syncthreads();
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+      const double v = (j == k) ? 1.0 : A[k + (size_t)j * ld];
+      A[k + (size_t)j * ld] = v * pinv;
+    }
+    __syncthreads();
+    // eliminate column k from every other row
+    for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+      const int r = idx % N, j = idx / N;
+      if (r != k) {
+        const double f = colk[r];
+        const double base = (j == k) ? 0.0 : A[r + (size_t)j * ld];
+        A[r + (size_t)j * ld] = fma(-f, A[k + (size_t)j * ld], base);
+      }
+    }
+    __syncthreads();
+  }
+  // undo the row interchanges as column interchanges, in reverse order
+  for (int k = N - 1; k >= 0; --k) {
+    const int pr = perm[k];
+    if (pr != k) {
+      for (int r = threadIdx.x; r < N; r += blockDim.x) {
+        const double t0 = A[r + (size_t)k * ld];
+        A[r + (size_t)k * ld] = A[r + (size_t)pr * ld];
+        A[r + (size_t)pr * ld] = t0;
+      }
+    }
+    __syncthreads();
+  }
+  if (resident) copy_mat(src, N, A, ld, N);
+}
+
+// ---------------------------------------------------------------------------------
+//  k_gemm: batched C = alpha * op(A) diag(f(ks)) op(B) * rowscale * colscale + beta C.
+//  64 x 64 output tile per CTA, 4 warps (each 32 x 32 = 2 x 4 DMMA m16n8k4 tiles),
+//  k-chunks of 16 staged in shared memory.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ double vscale(const double* v, int mode, int i) {
+  if (!v || mode == 0) return 1.0;
+  const double x = v[i];
+  if (mode == 1) return x;
+  if (mode == 2) return 1.0 / fmax(x, 1.0);
+  return fmin(x, 1.0);
+}
+
+constexpr int GBM = 64, GBN = 64, GBK = 16, GLD = 68;
+
+__global__ void __launch_bounds__(128)
+k_gemm(const HqGemmJob* __restrict__ jobs, int njobs, int tiles_n) {
+  __shared__ __align__(16) double sA[GBK * GLD];
+  __shared__ __align__(16) double sB[GBK * GLD];
+  __shared__ double red[32];
+  const int jb = blockIdx.y;
+  if (jb >= njobs) return;
+  const HqGemmJob J = jobs[jb];
+  if (!J.active) return;
+  const int tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
+  const int m0 = tm * GBM, n0 = tn * GBN;
+  if (m0 >= J.M || n0 >= J.Nc) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+  double acc[2][4][4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = acc[a][b][2] = acc[a][b][3] = 0.0;
+  for (int k0 = 0; k0 < J.K; k0 += GBK) {
+    __syncthreads();
+    // op(A) tile: rows m0..m0+63, cols k0..k0+15 -> sA[k][m]
+    for (int idx = threadIdx.x; idx < GBM * GBK; idx += blockDim.x) {
+      int m, k;
+      if (!J.ta) { m = idx % GBM; k = idx / GBM; } else { k = idx % GBK; m = idx / GBK; }
+      const int gm = m0 + m, gk = k0 + k;
+      double v = 0.0;
+      if (gm < J.M && gk < J.K) {
+        v = !J.ta ? J.A[gm + (size_t)gk * J.lda] : J.A[gk + (size_t)gm * J.lda];
+        v *= vscale(J.ks, J.ks_mode, gk);
+      }
+      sA[k * GLD + m] = v;
+    }
+    // op(B) tile: rows k0..k0+15, cols n0..n0+63 -> sB[k][n]
+    for (int idx = threadIdx.x; idx < GBK * GBN; idx += blockDim.x) {
+      int k, n;
+      if (!J.tb) { k = idx % GBK; n = idx / GBK; } else { n = idx % GBN; k = idx / GBN; }
+      const int gk = k0 + k, gn = n0 + n;
+      double v = 0.0;
+      if (gk < J.K && gn < J.Nc) v = !J.tb ? J.B[gk + (size_t)gn * J.ldb] : J.B[gn + (size_t)gk * J.ldb];
+      sB[k * GLD + n] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GBK; kk += 4) {
+      double a[2][2], bb[4];
+#pragma unroll
+      for (int a_ = 0; a_ < 2; ++a_) {
+        a[a_][0] = sA[(kk + q) * GLD + wm + a_ * 16 + g];
+        a[a_][1] = sA[(kk + q) * GLD + wm + a_ * 16 + g + 8];
+      }
+#pragma unroll
+      for (int b_ = 0; b_ < 4; ++b_) bb[b_] = sB[(kk + q) * GLD + wn + b_ * 8 + g];
+#pragma unroll
+      for (int a_ = 0; a_ < 2; ++a_)
+#pragma unroll
+        for (int b_ = 0; b_ < 4; ++b_) dmma_16x8x4(acc[a_][b_], a[a_][0], a[a_][1], bb[b_]);
+    }
+  }
+  // epilogue
+  double emax = -INFINITY;
+#pragma unroll
+  for (int a_ = 0; a_ < 2; ++a_)
+#pragma unroll
+    for (int b_ = 0; b_ < 4; ++b_)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int gm = m0 + wm + a_ * 16 + g + ((e & 2) ? 8 : 0);
+        const int gn = n0 + wn + b_ * 8 + 2 * q + (e & 1);
+        if (gm < J.M && gn < J.Nc) {
+          double v = J.alpha * acc[a_][b_][e] * vscale(J.rs, J.rs_mode, gm) * vscale(J.cs, J.cs_mode, gn);
+          double* cp = J.C + gm + (size_t)gn * J.ldc;
+          const double old = (J.beta != 0.0 || J.epi == 1) ? *cp : 0.0;
+          if (J.beta != 0.0) v = fma(J.beta, old, v);
+          if (J.epi == 1) emax = fmax(emax, v - old);
+          *cp = v;
+        }
+      }
+  if (J.epi == 1 && J.err_out) {
+    emax = block_max(emax, red);
+    if (threadIdx.x == 0) atomic_max_double(J.err_out, emax);
+  }
+}
+
+// ---------------------------------------------------------------------------------
+//  k_measure: estimators + snapshot of G after a stabilisation (slice `lslice`
+//  computed from the interval), the last slice of every interval.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(HQ_THREADS)
+k_measure(const HqChain* __restrict__ chains, int nchains, int dir, int b, int flags) {
+  __shared__ HqChain ch;
+  __shared__ double red[32];
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  if (threadIdx.x == 0) ch = chains[c];
+  __syncthreads();
+  if (!ch.active || b >= ch.n_stab) return;
+  const int N = ch.N;
+  int t_lo, t_hi;
+  interval_range(ch.nt, ch.pace, ch.n_stab, dir, b, t_lo, t_hi);
+  // up / dynamic: the last slice is t_hi, stored at t_hi % nt; down: t_lo, stored at t_lo - 1
+  const int lm = (dir == HQ_DOWN) ? ((t_lo - 1) % ch.nt) : (t_hi % ch.nt);
+  if (flags & HQ_F_MEASURE) measure_slice(ch.G, N, N, ch.acc, red);
+  if ((flags & HQ_F_SNAPSHOT) && ch.snap_tt) copy_mat(ch.snap_tt + (size_t)lm * N * N, N, ch.G, N, N);
+}
+
+// ---------------------------------------------------------------------------------
+//  Dynamic (time-displaced) sweep, src/dqmc_core.cpp:291-390. Per slice t:
+//    G(t,t) <- B G B^-1 ; G(t,0) <- B G(t,0) ; G(0,t) <- G(0,t) B^-1
+//  k_dyn_slices applies this for the interval's slices to one of the three matrices per
+//  CTA (blockIdx.y = 0: G(t,t), 1: G(t,0), 2: G(0,t)), except for the last slice which
+//  is rebuilt by the boundary step, and stores the per-slice results.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(HQ_THREADS, 1)
+k_dyn_slices(const HqChain* __restrict__ chains, int nchains, int b, int flags, int resident) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ HqChain ch;
+  __shared__ int8_t s[HQ_MAX_N];
+  const int c = blockIdx.x, which = blockIdx.y;
+  if (c >= nchains) return;
+  if (threadIdx.x == 0) ch = chains[c];
+  __syncthreads();
+  if (!ch.active || b >= ch.n_stab) return;
+  const int N = ch.N;
+  int t_lo, t_hi;
+  interval_range(ch.nt, ch.pace, ch.n_stab, HQ_UP, b, t_lo, t_hi);
+  double* src = which == 0 ? ch.G : (which == 1 ? ch.Gt0 : ch.G0t);
+  double* snap = which == 0 ? ch.snap_tt : (which == 1 ? ch.snap_t0 : ch.snap_0t);
+  double* M;
+  int ld;
+  double* p = smem;
+  if (resident) { M = p; ld = smem_ld(N); p += (size_t)N * ld; copy_mat(M, ld, src, N, N); }
+  else { M = src; ld = N; }
+  double* stage = p;
+  __syncthreads();
+  const int nsl = t_hi - t_lo + 1;
+  for (int step = 0; step < nsl; ++step) {
+    const int t = t_lo + step;
+    const int l = t % ch.nt;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s[i] = ch.fields[(size_t)l * N + i];
+    __syncthreads();
+    if (which != 2) {  // left multiplication by B(l) = e^V E
+      apply_expk(ch, M, ld, 0, false, stage);
+      scale_rows(M, ld, N, s, ch.ev_p, ch.ev_m);
+      __syncthreads();
+    }
+    if (which != 1) {  // right multiplication by B(l)^-1 = E^-1 e^-V
+      apply_expk(ch, M, ld, 1, true, stage);
+      scale_cols(M, ld, N, s, ch.ev_m, ch.ev_p);
+      __syncthreads();
+    }
+    if (step < nsl - 1 && snap) copy_mat(snap + (size_t)l * N * N, N, M, ld, N);
+    __syncthreads();
+  }
+  if (resident) copy_mat(src, N, M, ld, N);
+}
+
+// G(t,0) <- G(t,t) and G(0,t) <- G(t,t) - 1 at the start of a dynamic sweep
+// (src/dqmc_core.cpp:302-303)
+__global__ void k_dyn_start(const HqChain* __restrict__ chains, int nchains) {
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  const HqChain& ch = chains[c];
+  if (!ch.active) return;
+  const int N = ch.N;
+  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+    const int i = idx % N, j = idx / N;
+    const double v = ch.G[idx];
+    ch.Gt0[idx] = v;
+    ch.G0t[idx] = v - (i == j ? 1.0 : 0.0);
+  }
+}
+
+// dynamic estimators of one slice l from G(t,0), G(0,t) (include/observable_methods.hpp:
+// 110-120, 178-195) and the displacement-summed g(d) = sum_i G(t,0)[i+d, i] for G(k,t)
+// (:84-103). dyn_acc layout: [0][nt] spin, [1][nt] ldos, [2 + d][nt] g(d) for d < N.
+__device__ void dyn_measure(const HqChain& ch, const double* Gt0, const double* G0t, int l, double* red) {
+  const int N = ch.N, L = ch.L;
+  double sp = 0.0, ld = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const double a = Gt0[i + (size_t)i * N], b = G0t[i + (size_t)i * N];
+    sp -= 2.0 * a * b;
+    ld += a;
+  }
+  sp = block_sum(sp, red);
+  ld = block_sum(ld, red);
+  if (threadIdx.x == 0) {
+    ch.dyn_acc[0 * ch.nt + l] += sp / (2.0 * N);
+    ch.dyn_acc[1 * ch.nt + l] += ld / N;
+  }
+  // g(d): d = dx + L dy, sum over i of G[(xi+dx, yi+dy), i]
+  for (int d = threadIdx.x; d < N; d += blockDim.x) {
+    const int dx = d % L, dy = d / L;
+    double acc = 0.0;
+    for (int i = 0; i < N; ++i) {
+      const int xi = i % L, yi = i / L;
+      const int j = (xi + dx) % L + L * ((yi + dy) % L);
+      acc += Gt0[j + (size_t)i * N];
+    }
+    ch.dyn_acc[(size_t)(2 + d) * ch.nt + l] += acc;
+  }
+}
+
+// measure the dynamic estimators of every slice of interval b from the snapshots
+// (slices of the interval other than the last) or from the fresh G's (the last one).
+__global__ void __launch_bounds__(HQ_THREADS)
+k_dyn_measure(const HqChain* __restrict__ chains, int nchains, int b, int last_only) {
+  __shared__ HqChain ch;
+  __shared__ double red[32];
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  if (threadIdx.x == 0) ch = chains[c];
+  __syncthreads();
+  if (!ch.active || b >= ch.n_stab) return;
+  const int N = ch.N;
+  int t_lo, t_hi;
+  interval_range(ch.nt, ch.pace, ch.n_stab, HQ_UP, b, t_lo, t_hi);
+  const size_t NN = (size_t)N * N;
+  for (int t = last_only ? t_hi : t_lo; t <= t_hi; ++t) {
+    const int l = t % ch.nt;
+    const double* gt0;
+    const double* g0t;
+    if (t == t_hi) { gt0 = ch.Gt0; g0t = ch.G0t; }
+    else { gt0 = ch.snap_t0 + l * NN; g0t = ch.snap_0t + l * NN; }
+    dyn_measure(ch, gt0, g0t, l, red);
+    __syncthreads();
+  }
+}
+
+// at a dynamic boundary: copy the fresh G's into the snapshots of the boundary slice
+// with the tau = 0 convention (src/dqmc_core.cpp:379-387)
+__global__ void k_dyn_store(const HqChain* __restrict__ chains, int nchains, int b) {
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  const HqChain& ch = chains[c];
+  if (!ch.active || b >= ch.n_stab) return;
+  const int N = ch.N;
+  int t_lo, t_hi;
+  interval_range(ch.nt, ch.pace, ch.n_stab, HQ_UP, b, t_lo, t_hi);
+  const int l = t_hi % ch.nt;
+  const size_t NN = (size_t)N * N;
+  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+    const int i = idx % N, j = idx / N;
+    const double gtt = ch.G[idx];
+    if (ch.snap_tt) ch.snap_tt[l * NN + idx] = gtt;
+    if (l == 0) {
+      // at tau = beta the stored pair is G(0,0), G(0,0) - 1; the propagated matrices
+      // are replaced likewise
+      ch.Gt0[idx] = gtt;
+      ch.G0t[idx] = gtt - (i == j ? 1.0 : 0.0);
+    }
+    if (ch.snap_t0) ch.snap_t0[l * NN + idx] = ch.Gt0[idx];
+    if (ch.snap_0t) ch.snap_0t[l * NN + idx] = ch.G0t[idx];
+  }
+}
+
+// commit the freshly built G(t,t), G(t,0), G(0,t) (in W3, W0, W5) after recording the
+// signed wrap errors (src/dqmc_core.cpp:334-344)
+__global__ void __launch_bounds__(HQ_THREADS) k_dyn_commit(const HqChain* __restrict__ chains, int nchains, int b) {
+  __shared__ double red[32];
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  const HqChain& ch = chains[c];
+  if (!ch.active || b >= ch.n_stab) return;
+  const int NN = ch.N * ch.N;
+  double ett = -INFINITY, edyn = -INFINITY;
+  for (int idx = threadIdx.x; idx < NN; idx += blockDim.x) {
+    const double ftt = ch.W3[idx], ft0 = ch.W0[idx], f0t = ch.W4[idx];
+    ett = fmax(ett, ftt - ch.G[idx]);
+    edyn = fmax(edyn, fmax(ft0 - ch.Gt0[idx], f0t - ch.G0t[idx]));
+    ch.G[idx] = ftt;
+    ch.Gt0[idx] = ft0;
+    ch.G0t[idx] = f0t;
+  }
+  ett = block_max(ett, red);
+  edyn = block_max(edyn, red);
+  if (threadIdx.x == 0) {
+    ch.acc[HQ_ACC_WRAP_TT] = fmax(ch.acc[HQ_ACC_WRAP_TT], ett);
+    ch.acc[HQ_ACC_WRAP_DYN] = fmax(ch.acc[HQ_ACC_WRAP_DYN], edyn);
+  }
+}
+
+// ---------------------------------------------------------------------------------
+//  Adjoint of log|det(1 + B(nt-1)...B(0))| (no counterpart in the reference).
+//  With G_l = (1 + B_l..B_1 B_nt..B_{l+1})^-1 the G of the up sweep after slice l:
+//    d/dmu    = dt sum_l tr(1 - G_l)
+//    d/dalpha = sum_l sum_i s_li (1 - G_l)_ii
+//    d/dE     : tr(dE E^-1 D),  D = sum_l e^{-V_l} (1 - G_l) e^{V_l}
+//  A no-update up pass wraps G slice by slice and is rebuilt from the stacks every
+//  `pace` slices (the checkpoints), so no slice is stored. D accumulates in W4.
+// ---------------------------------------------------------------------------------
+__device__ void adj_accum(const HqChain& ch, const double* G, int ld, const int8_t* s, double* red) {
+  const int N = ch.N;
+  double tr = 0.0, sa = 0.0;
+  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
+    const int i = idx % N, j = idx / N;
+    const double one_m = (i == j ? 1.0 : 0.0) - G[i + (size_t)j * ld];
+    const double f = (s[i] > 0 ? ch.ev_m : ch.ev_p) * (s[j] > 0 ? ch.ev_p : ch.ev_m);
+    ch.W4[idx] += one_m * f;
+    if (i == j) { tr += one_m; sa += (s[i] > 0 ? one_m : -one_m); }
+  }
+  tr = block_sum(tr, red);
+  sa = block_sum(sa, red);
+  if (threadIdx.x == 0) {
+    ch.acc[HQ_ACC_DMU] += ch.dt * tr;
+    ch.acc[HQ_ACC_DALPHA] += sa;
+  }
+}
+
+__global__ void __launch_bounds__(HQ_THREADS, 1)
+k_adj_interval(const HqChain* __restrict__ chains, int nchains, int b, int resident) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ HqChain ch;
+  __shared__ double red[32];
+  __shared__ int8_t s[HQ_MAX_N];
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  if (threadIdx.x == 0) ch = chains[c];
+  __syncthreads();
+  if (!ch.active || b >= ch.n_stab) return;
+  const int N = ch.N;
+  int t_lo, t_hi;
+  interval_range(ch.nt, ch.pace, ch.n_stab, HQ_UP, b, t_lo, t_hi);
+  double* G;
+  int ld;
+  double* p = smem;
+  if (resident) { G = p; ld = smem_ld(N); p += (size_t)N * ld; copy_mat(G, ld, ch.G, N, N); }
+  else { G = ch.G; ld = N; }
+  double* stage = p;
+  __syncthreads();
+  const int nsl = t_hi - t_lo + 1;
+  for (int step = 0; step < nsl; ++step) {
+    const int t = t_lo + step;
+    const int l = t % ch.nt;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s[i] = ch.fields[(size_t)l * N + i];
+    __syncthreads();
+    wrap_slice(ch, G, ld, s, HQ_UP, stage);
+    if (step < nsl - 1) adj_accum(ch, G, ld, s, red);
+    __syncthreads();
+  }
+  if (resident) copy_mat(ch.G, N, G, ld, N);
+}
+
+// the last slice of interval b, after the boundary rebuilt G
+__global__ void __launch_bounds__(HQ_THREADS) k_adj_last(const HqChain* __restrict__ chains, int nchains, int b) {
+  __shared__ HqChain ch;
+  __shared__ double red[32];
+  __shared__ int8_t s[HQ_MAX_N];
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  if (threadIdx.x == 0) ch = chains[c];
+  __syncthreads();
+  if (!ch.active || b >= ch.n_stab) return;
+  const int N = ch.N;
+  int t_lo, t_hi;
+  interval_range(ch.nt, ch.pace, ch.n_stab, HQ_UP, b, t_lo, t_hi);
+  const int l = t_hi % ch.nt;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) s[i] = ch.fields[(size_t)l * N + i];
+  __syncthreads();
+  adj_accum(ch, ch.G, N, s, red);
+}
+
+}  // namespace hq
+
+// =====================================================================================
+//  launch wrappers (host)
+// =====================================================================================
+namespace hq {
+
+size_t smem_interval_bytes(int Nmax, int kmax, bool resident) {
+  return interval_smem_doubles(Nmax, kmax, resident) * sizeof(double);
+}
+size_t smem_matrix_bytes(int Nmax, bool resident, int extra_doubles) {
+  const size_t mat = resident ? (size_t)Nmax * smem_ld(Nmax) : 0;
+  return (mat + (size_t)extra_doubles) * sizeof(double);
+}
+
+static cudaError_t set_smem(const void* fn, size_t bytes) {
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// sets the dynamic shared-memory limits of every per-chain kernel once (outside any
+// stream capture) for the largest chain of a context
+cudaError_t prepare_kernels(int Nmax, int kmax, bool resident) {
+  const size_t mat_stage = smem_matrix_bytes(Nmax, resident, 8 * (((Nmax + 15) & ~15) + 4) + 64);
+  cudaError_t e;
+  if ((e = set_smem((const void*)k_interval, smem_interval_bytes(Nmax, kmax, resident))) != cudaSuccess) return e;
+  if ((e = set_smem((const void*)k_bchain, mat_stage)) != cudaSuccess) return e;
+  if ((e = set_smem((const void*)k_udt, smem_matrix_bytes(Nmax, resident, 5 * Nmax + 64))) != cudaSuccess) return e;
+  if ((e = set_smem((const void*)k_invert, smem_matrix_bytes(Nmax, resident, 2 * Nmax + 64))) != cudaSuccess) return e;
+  if ((e = set_smem((const void*)k_dyn_slices, mat_stage)) != cudaSuccess) return e;
+  if ((e = set_smem((const void*)k_adj_interval, mat_stage)) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+cudaError_t launch_interval(const HqChain* chains, int n, int dir, int b, int flags, int Nmax, int kmax, bool resident,
+                            cudaStream_t st) {
+  const size_t bytes = smem_interval_bytes(Nmax, kmax, resident);
+  k_interval<<<n, HQ_THREADS, bytes, st>>>(chains, n, dir, b, flags, resident ? 1 : 0);
+  return cudaGetLastError();
+}
+cudaError_t launch_bchain(const HqChain* chains, int n, int dir, int b, int Nmax, bool resident, cudaStream_t st) {
+  const size_t bytes = smem_matrix_bytes(Nmax, resident, 8 * (((Nmax + 15) & ~15) + 4) + 64);
+  k_bchain<<<n, HQ_THREADS, bytes, st>>>(chains, n, dir, b, resident ? 1 : 0);
+  return cudaGetLastError();
+}
+cudaError_t launch_udt(const HqChain* chains, int n, int side, int b, int Nmax, bool resident, cudaStream_t st) {
+  const size_t bytes = smem_matrix_bytes(Nmax, resident, 5 * Nmax + 64);
+  k_udt<<<n, HQ_THREADS, bytes, st>>>(chains, n, side, 0, b, resident ? 1 : 0);
+  return cudaGetLastError();
+}
+cudaError_t launch_invert(const HqChain* chains, int n, int b, int which, int Nmax, bool resident, cudaStream_t st) {
+  const size_t bytes = smem_matrix_bytes(Nmax, resident, 2 * Nmax + 64);
+  k_invert<<<n, HQ_THREADS, bytes, st>>>(chains, n, b, which, resident ? 1 : 0);
+  return cudaGetLastError();
+}
+cudaError_t launch_gemm(const HqGemmJob* jobs, int njobs, int Mmax, int Nmax, cudaStream_t st) {
+  if (njobs <= 0) return cudaSuccess;
+  const int tm = (Mmax + GBM - 1) / GBM, tn = (Nmax + GBN - 1) / GBN;
+  dim3 grid(tm * tn, njobs);
+  k_gemm<<<grid, 128, 0, st>>>(jobs, njobs, tn);
+  return cudaGetLastError();
+}
+cudaError_t launch_measure(const HqChain* chains, int n, int dir, int b, int flags, cudaStream_t st) {
+  k_measure<<<n, HQ_THREADS, 0, st>>>(chains, n, dir, b, flags);
+  return cudaGetLastError();
+}
+cudaError_t launch_dyn_start(const HqChain* chains, int n, cudaStream_t st) {
+  k_dyn_start<<<n, 256, 0, st>>>(chains, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_dyn_slices(const HqChain* chains, int n, int b, int flags, int Nmax, bool resident, cudaStream_t st) {
+  const size_t bytes = smem_matrix_bytes(Nmax, resident, 8 * (((Nmax + 15) & ~15) + 4) + 64);
+  dim3 grid(n, 3);
+  k_dyn_slices<<<grid, HQ_THREADS, bytes, st>>>(chains, n, b, flags, resident ? 1 : 0);
+  return cudaGetLastError();
+}
+cudaError_t launch_dyn_measure(const HqChain* chains, int n, int b, int last_only, cudaStream_t st) {
+  k_dyn_measure<<<n, HQ_THREADS, 0, st>>>(chains, n, b, last_only);
+  return cudaGetLastError();
+}
+cudaError_t launch_dyn_store(const HqChain* chains, int n, int b, cudaStream_t st) {
+  k_dyn_store<<<n, 256, 0, st>>>(chains, n, b);
+  return cudaGetLastError();
+}
+cudaError_t launch_adj_interval(const HqChain* chains, int n, int b, int Nmax, bool resident, cudaStream_t st) {
+  const size_t bytes = smem_matrix_bytes(Nmax, resident, 8 * (((Nmax + 15) & ~15) + 4) + 64);
+  k_adj_interval<<<n, HQ_THREADS, bytes, st>>>(chains, n, b, resident ? 1 : 0);
+  return cudaGetLastError();
+}
+cudaError_t launch_adj_last(const HqChain* chains, int n, int b, cudaStream_t st) {
+  k_adj_last<<<n, HQ_THREADS, 0, st>>>(chains, n, b);
+  return cudaGetLastError();
+}
+cudaError_t launch_dyn_commit(const HqChain* chains, int n, int b, cudaStream_t st) {
+  k_dyn_commit<<<n, HQ_THREADS, 0, st>>>(chains, n, b);
+  return cudaGetLastError();
+}
+
+}  // namespace hq

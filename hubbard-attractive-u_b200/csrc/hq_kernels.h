@@ -1,0 +1,25 @@
+// hq_kernels.h -- host-side launch wrappers of the sm_100a DQMC kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include "hq_types.h"
+
+namespace hq {
+size_t smem_interval_bytes(int Nmax, int kmax, bool resident);
+size_t smem_matrix_bytes(int Nmax, bool resident, int extra_doubles);
+cudaError_t prepare_kernels(int Nmax, int kmax, bool resident);
+cudaError_t launch_interval(const HqChain* chains, int n, int dir, int b, int flags, int Nmax, int kmax, bool resident,
+                            cudaStream_t st);
+cudaError_t launch_bchain(const HqChain* chains, int n, int dir, int b, int Nmax, bool resident, cudaStream_t st);
+cudaError_t launch_udt(const HqChain* chains, int n, int side, int b, int Nmax, bool resident, cudaStream_t st);
+cudaError_t launch_invert(const HqChain* chains, int n, int b, int which, int Nmax, bool resident, cudaStream_t st);
+cudaError_t launch_gemm(const HqGemmJob* jobs, int njobs, int Mmax, int Nmax, cudaStream_t st);
+cudaError_t launch_measure(const HqChain* chains, int n, int dir, int b, int flags, cudaStream_t st);
+cudaError_t launch_dyn_start(const HqChain* chains, int n, cudaStream_t st);
+cudaError_t launch_dyn_slices(const HqChain* chains, int n, int b, int flags, int Nmax, bool resident, cudaStream_t st);
+cudaError_t launch_dyn_measure(const HqChain* chains, int n, int b, int last_only, cudaStream_t st);
+cudaError_t launch_dyn_store(const HqChain* chains, int n, int b, cudaStream_t st);
+cudaError_t launch_dyn_commit(const HqChain* chains, int n, int b, cudaStream_t st);
+cudaError_t launch_adj_interval(const HqChain* chains, int n, int b, int Nmax, bool resident, cudaStream_t st);
+cudaError_t launch_adj_last(const HqChain* chains, int n, int b, cudaStream_t st);
+}  // namespace hq
