@@ -92,6 +92,24 @@ __device__ inline double block_max(double v, double* red) {
   return t;
 }
 
+// three block-wide sums in one reduction round (2 barriers)
+__device__ inline void block_sum3(double& a, double& b, double& c, double* red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  a = warp_sum(a); b = warp_sum(b); c = warp_sum(c);
+  __syncthreads();
+  if (lane == 0) { red[w] = a; red[32 + w] = b; red[64 + w] = c; }
+  __syncthreads();
+  a = warp_sum(lane < nw ? red[lane] : 0.0);
+  b = warp_sum(lane < nw ? red[32 + lane] : 0.0);
+  c = warp_sum(lane < nw ? red[64 + lane] : 0.0);
+}
+
+// Element loops over an N x N column-major matrix without integer division: warps walk
+// the columns, lanes the rows (consecutive lanes touch consecutive addresses).
+#define HQ_FOR_EACH_ELEM(N, i, j)                                                      \
+  for (int j = (int)(threadIdx.x >> 5); j < (N); j += (int)(blockDim.x >> 5))          \
+    for (int i = (int)(threadIdx.x & 31); i < (N); i += 32)
+
 // atomic max on doubles (ordered-int trick; values may be negative)
 __device__ inline void atomic_max_double(double* addr, double val) {
   unsigned long long* p = reinterpret_cast<unsigned long long*>(addr);
@@ -111,61 +129,63 @@ __device__ inline void atomic_max_double(double* addr, double val) {
 //  side 0: M <- c (A(x)A) M  (rows);  side 1: M <- c M (A(x)A)  (columns).
 //  rows/cols outside [0, N) are untouched. All threads of the block participate.
 // ------------------------------------------------------------------------------------
-template <int LT>
-__device__ inline void sep_pass(double* M, int ld, int N, int L, const double* __restrict__ a, double c, int side,
+template <int L>
+__device__ inline void sep_pass(double* M, int ld, int N, const double* __restrict__ coef, double c, int side,
                                 int pass) {
-  // a fiber: fixed (other coordinate, matrix index); LT = compile-time bound on L
-  const int nfib = N * L;  // (N matrices-lines) x (L fibers per line)
+  // circulant coefficients in registers (compile-time indices after unrolling)
+  double a[L];
+#pragma unroll
+  for (int d = 0; d < L; ++d) a[d] = coef[d];
+  const int nfib = N * L;  // N lines (columns for side 0, rows for side 1) x L fibers each
   for (int f = threadIdx.x; f < nfib; f += blockDim.x) {
     const int line = f % N;   // column j (side 0) or row i (side 1)
-    const int o = f / N;      // the fixed coordinate of the fiber
-    double v[LT];
-    // element offset of fiber entry e (0 <= e < L)
-    // side 0 (rows, column `line`):  i = x + L y ; pass 0 runs over x with y = o, pass 1 over y with x = o
-    // side 1 (columns, row `line`):  j = x + L y ; same
+    const int o = f / N;      // the fixed lattice coordinate of the fiber
+    // pass 0 runs over x with y = o (sites L*o + e); pass 1 over y with x = o (sites o + L*e)
     const int base_site = (pass == 0) ? (L * o) : o;
     const int step_site = (pass == 0) ? 1 : L;
+    double* base = (side == 0) ? (M + base_site + (size_t)line * ld) : (M + line + (size_t)base_site * ld);
+    const size_t stride = (side == 0) ? (size_t)step_site : (size_t)step_site * ld;
+    double v[L];
 #pragma unroll
-    for (int e = 0; e < LT; ++e) {
-      if (e < L) {
-        const int s = base_site + e * step_site;
-        v[e] = (side == 0) ? M[s + (size_t)line * ld] : M[line + (size_t)s * ld];
-      }
-    }
+    for (int e = 0; e < L; ++e) v[e] = base[e * stride];
 #pragma unroll
-    for (int e = 0; e < LT; ++e) {
-      if (e < L) {
-        double acc = 0.0;
+    for (int e = 0; e < L; ++e) {
+      double acc = 0.0;
 #pragma unroll
-        for (int e2 = 0; e2 < LT; ++e2) {
-          if (e2 < L) {
-            int d = e - e2;
-            d += (d < 0) ? L : 0;
-            acc = fma(a[d], v[e2], acc);
-          }
-        }
-        if (pass == 1) acc *= c;
-        const int s = base_site + e * step_site;
-        if (side == 0) M[s + (size_t)line * ld] = acc; else M[line + (size_t)s * ld] = acc;
-      }
+      for (int e2 = 0; e2 < L; ++e2) acc = fma(a[(e - e2 + L) % L], v[e2], acc);
+      base[e * stride] = (pass == 1) ? acc * c : acc;
     }
   }
 }
 
-template <int LT>
-__device__ inline void sep_apply(double* M, int ld, int N, int L, const double* a, double c, int side) {
-  sep_pass<LT>(M, ld, N, L, a, c, side, 0);
+template <int L>
+__device__ inline void sep_apply(double* M, int ld, int N, const double* a, double c, int side) {
+  sep_pass<L>(M, ld, N, a, c, side, 0);
   __syncthreads();
-  sep_pass<LT>(M, ld, N, L, a, c, side, 1);
+  sep_pass<L>(M, ld, N, a, c, side, 1);
   __syncthreads();
 }
 
-// dispatch on L to a compile-time fiber length
+// dispatch on the lattice size to an exact compile-time fiber length (L <= HQ_MAX_L)
 __device__ inline void sep_apply_any(double* M, int ld, int N, int L, const double* a, double c, int side) {
-  if (L <= 4) sep_apply<4>(M, ld, N, L, a, c, side);
-  else if (L <= 8) sep_apply<8>(M, ld, N, L, a, c, side);
-  else if (L <= 12) sep_apply<12>(M, ld, N, L, a, c, side);
-  else sep_apply<16>(M, ld, N, L, a, c, side);
+  switch (L) {
+    case 1: sep_apply<1>(M, ld, N, a, c, side); break;
+    case 2: sep_apply<2>(M, ld, N, a, c, side); break;
+    case 3: sep_apply<3>(M, ld, N, a, c, side); break;
+    case 4: sep_apply<4>(M, ld, N, a, c, side); break;
+    case 5: sep_apply<5>(M, ld, N, a, c, side); break;
+    case 6: sep_apply<6>(M, ld, N, a, c, side); break;
+    case 7: sep_apply<7>(M, ld, N, a, c, side); break;
+    case 8: sep_apply<8>(M, ld, N, a, c, side); break;
+    case 9: sep_apply<9>(M, ld, N, a, c, side); break;
+    case 10: sep_apply<10>(M, ld, N, a, c, side); break;
+    case 11: sep_apply<11>(M, ld, N, a, c, side); break;
+    case 12: sep_apply<12>(M, ld, N, a, c, side); break;
+    case 13: sep_apply<13>(M, ld, N, a, c, side); break;
+    case 14: sep_apply<14>(M, ld, N, a, c, side); break;
+    case 15: sep_apply<15>(M, ld, N, a, c, side); break;
+    default: sep_apply<16>(M, ld, N, a, c, side); break;
+  }
 }
 
 // ------------------------------------------------------------------------------------
@@ -199,11 +219,11 @@ __device__ inline void dense_apply(double* M, int ld, int N, const double* __res
     for (int k0 = 0; k0 < N; k0 += 8) {
       // stage[kk * lds + r] = E[r, k0 + kk]
       __syncthreads();
-      for (int idx = threadIdx.x; idx < 8 * N16; idx += blockDim.x) {
-        const int kk = idx / N16, r = idx % N16;
-        const int k = k0 + kk;
-        stage[kk * lds + r] = (r < N && k < N) ? E[r + (size_t)k * N] : 0.0;
-      }
+      for (int kk = threadIdx.x >> 5; kk < 8; kk += blockDim.x >> 5)
+        for (int r = threadIdx.x & 31; r < N16; r += 32) {
+          const int k = k0 + kk;
+          stage[kk * lds + r] = (r < N && k < N) ? E[r + (size_t)k * N] : 0.0;
+        }
       __syncthreads();
 #pragma unroll
       for (int f = 0; f < kMaxFrag; ++f) {
@@ -264,11 +284,11 @@ __device__ inline void dense_apply_right(double* M, int ld, int N, const double*
     for (int k0 = 0; k0 < N; k0 += 8) {
       __syncthreads();
       // stage[kk * lds + c] = E[k0+kk, c]
-      for (int idx = threadIdx.x; idx < 8 * N8; idx += blockDim.x) {
-        const int kk = idx / N8, c = idx % N8;
-        const int k = k0 + kk;
-        stage[kk * lds + c] = (c < N && k < N) ? E[k + (size_t)c * N] : 0.0;
-      }
+      for (int kk = threadIdx.x >> 5; kk < 8; kk += blockDim.x >> 5)
+        for (int c = threadIdx.x & 31; c < N8; c += 32) {
+          const int k = k0 + kk;
+          stage[kk * lds + c] = (c < N && k < N) ? E[k + (size_t)c * N] : 0.0;
+        }
       __syncthreads();
 #pragma unroll
       for (int f = 0; f < kMaxFrag; ++f) {
@@ -307,27 +327,25 @@ __device__ inline void dense_apply_right(double* M, int ld, int N, const double*
 
 // M <- diag(v) M (rows) with v_i = (s_i > 0 ? vp : vm) ; fields is the slice's int8 row
 __device__ inline void scale_rows(double* M, int ld, int N, const int8_t* s, double vp, double vm) {
-  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-    const int i = idx % N, j = idx / N;
-    M[i + (size_t)j * ld] *= (s[i] > 0 ? vp : vm);
-  }
+  HQ_FOR_EACH_ELEM(N, i, j) M[i + (size_t)j * ld] *= (s[i] > 0 ? vp : vm);
 }
 // M <- M diag(v) (columns)
 __device__ inline void scale_cols(double* M, int ld, int N, const int8_t* s, double vp, double vm) {
-  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-    const int i = idx % N, j = idx / N;
-    M[i + (size_t)j * ld] *= (s[j] > 0 ? vp : vm);
-  }
+  HQ_FOR_EACH_ELEM(N, i, j) M[i + (size_t)j * ld] *= (s[j] > 0 ? vp : vm);
 }
 
 // M <- expK M   (side 0)  /  M <- M expK (side 1); inv selects inv_expK
 __device__ inline void apply_expk(const HqChain& ch, double* M, int ld, int side, bool inv, double* stage) {
   if (ch.expk_mode == HQK_EXPK_SEPARABLE) {
+#ifndef HQ_TEST_NO_SEP
     sep_apply_any(M, ld, ch.N, ch.L, inv ? ch.sep_ai : ch.sep_a, inv ? ch.sep_ci : ch.sep_c, side);
+#endif
   } else {
+#ifndef HQ_TEST_NO_DENSE
     const double* E = inv ? ch.inv_expK : ch.expK;
     if (side == 0) dense_apply(M, ld, ch.N, E, stage);
     else dense_apply_right(M, ld, ch.N, E, stage);
+#endif
   }
 }
 

@@ -514,7 +514,7 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   c->resident = hq::smem_interval_bytes(c->Nmax, 4, true) <= budget &&
                 hq::smem_matrix_bytes(c->Nmax, true, 8 * (((c->Nmax + 15) & ~15) + 4) + 64) <= budget;
   int kfit = 4;
-  for (int k : {64, 32, 16, 8, 4})
+  for (int k : {16, 8, 4})
     if (hq::smem_interval_bytes(c->Nmax, k, c->resident) <= budget) { kfit = k; break; }
   for (int i = 0; i < n_chains; ++i) {
     ChainHost& h = c->ch[i];

@@ -29,11 +29,15 @@ namespace hq {
 // consecutive columns hit distinct banks
 __host__ __device__ inline int smem_ld(int N) { return (N % 2 == 0) ? N + 1 : N; }
 
+// leading dimension of the delayed-update panels: = 4 (mod 16) doubles, so that the DMMA
+// fragment loads of the flush are free of bank conflicts
+__host__ __device__ inline int panel_ld(int N) { return N + ((4 - N % 16) + 16) % 16; }
+
 // bytes of dynamic shared memory of k_interval / k_bchain for a chain of size N with
 // delay depth kmax (matrix in smem when `resident`)
 __host__ __device__ inline size_t interval_smem_doubles(int N, int kmax, bool resident) {
   const size_t mat = resident ? (size_t)N * smem_ld(N) : 0;
-  const size_t panels = (size_t)N * kmax * 2;
+  const size_t panels = (size_t)panel_ld(N) * kmax * 2;
   const size_t stage = (size_t)8 * (((N + 15) & ~15) + 4);
   const size_t work = panels > stage ? panels : stage;
   return mat + work + 3 * (size_t)N + (size_t)(N + 7) / 4 + 64;
@@ -50,15 +54,12 @@ struct SliceView {
 // ---------------------------------------------------------------------------------
 __device__ void measure_slice(const double* G, int ld, int N, double* acc, double* red) {
   double tr = 0.0, dd = 0.0, sq = 0.0;
-  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-    const int i = idx % N, j = idx / N;
+  HQ_FOR_EACH_ELEM(N, i, j) {
     const double v = G[i + (size_t)j * ld];
-    sq += v * v;
+    sq = fma(v, v, sq);
     if (i == j) { tr += v; dd += (1.0 - v) * (1.0 - v); }
   }
-  tr = block_sum(tr, red);
-  dd = block_sum(dd, red);
-  sq = block_sum(sq, red);
+  block_sum3(tr, dd, sq, red);
   if (threadIdx.x == 0) {
     acc[HQ_ACC_FILLING] += 2.0 - 2.0 * tr / N;
     acc[HQ_ACC_DOCC] += dd / N;
@@ -68,10 +69,7 @@ __device__ void measure_slice(const double* G, int ld, int N, double* acc, doubl
 }
 
 __device__ void copy_mat(double* dst, int ldd, const double* src, int lds, int N) {
-  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-    const int i = idx % N, j = idx / N;
-    dst[i + (size_t)j * ldd] = src[i + (size_t)j * lds];
-  }
+  HQ_FOR_EACH_ELEM(N, i, j) dst[i + (size_t)j * ldd] = src[i + (size_t)j * lds];
 }
 
 // ---------------------------------------------------------------------------------
@@ -86,32 +84,48 @@ __device__ void copy_mat(double* dst, int ldd, const double* src, int lds, int N
 //  with DMMA when k reaches kmax and at the end of the slice.
 // ---------------------------------------------------------------------------------
 __device__ void flush_panels(double* G, int ld, int N, const double* X, int ldx, const double* Y, int ldy, int k) {
+  // G += X Y by 16 x 32 strips (four 16 x 8 DMMA tiles sharing the A fragments)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int g = lane >> 2, q = lane & 3;
-  const int mt = (N + 15) / 16, nt8 = (N + 7) / 8;
-  const int tiles = mt * nt8;
-  for (int tile = warp; tile < tiles; tile += nwarps) {
-    const int r0 = (tile % mt) * 16, c0 = (tile / mt) * 8;
-    const int r = r0 + g, c = c0 + 2 * q;
-    double acc[4];
-    acc[0] = (r < N && c < N) ? G[r + (size_t)c * ld] : 0.0;
-    acc[1] = (r < N && c + 1 < N) ? G[r + (size_t)(c + 1) * ld] : 0.0;
-    acc[2] = (r + 8 < N && c < N) ? G[r + 8 + (size_t)c * ld] : 0.0;
-    acc[3] = (r + 8 < N && c + 1 < N) ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
+  const int mt = (N + 15) / 16, ns = (N + 31) / 32;
+  const int strips = mt * ns;
+  for (int st = warp; st < strips; st += nwarps) {
+    const int r0 = (st % mt) * 16, c0 = (st / mt) * 32;
+    const int r = r0 + g;
+    double acc[4][4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int c = c0 + t * 8 + 2 * q;
+      acc[t][0] = (r < N && c < N) ? G[r + (size_t)c * ld] : 0.0;
+      acc[t][1] = (r < N && c + 1 < N) ? G[r + (size_t)(c + 1) * ld] : 0.0;
+      acc[t][2] = (r + 8 < N && c < N) ? G[r + 8 + (size_t)c * ld] : 0.0;
+      acc[t][3] = (r + 8 < N && c + 1 < N) ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
+    }
     for (int m0 = 0; m0 < k; m0 += 4) {
       const int m = m0 + q;
-      const double a0 = (r < N && m < k) ? X[r + m * ldx] : 0.0;
-      const double a1 = (r + 8 < N && m < k) ? X[r + 8 + m * ldx] : 0.0;
-      const int cb = c0 + g;
-      const double b0 = (cb < N && m < k) ? Y[m * ldy + cb] : 0.0;
-      dmma_16x8x4(acc, a0, a1, b0);
+      const bool mk = m < k;
+      const double a0 = (r < N && mk) ? X[r + m * ldx] : 0.0;
+      const double a1 = (r + 8 < N && mk) ? X[r + 8 + m * ldx] : 0.0;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int cb = c0 + t * 8 + g;
+        const double b0 = (cb < N && mk) ? Y[m * ldy + cb] : 0.0;
+        dmma_16x8x4(acc[t], a0, a1, b0);
+      }
     }
-    if (r < N && c < N) G[r + (size_t)c * ld] = acc[0];
-    if (r < N && c + 1 < N) G[r + (size_t)(c + 1) * ld] = acc[1];
-    if (r + 8 < N && c < N) G[r + 8 + (size_t)c * ld] = acc[2];
-    if (r + 8 < N && c + 1 < N) G[r + 8 + (size_t)(c + 1) * ld] = acc[3];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int c = c0 + t * 8 + 2 * q;
+      if (r < N && c < N) G[r + (size_t)c * ld] = acc[t][0];
+      if (r < N && c + 1 < N) G[r + (size_t)(c + 1) * ld] = acc[t][1];
+      if (r + 8 < N && c < N) G[r + 8 + (size_t)c * ld] = acc[t][2];
+      if (r + 8 < N && c + 1 < N) G[r + 8 + (size_t)(c + 1) * ld] = acc[t][3];
+    }
   }
 }
+
+// barrier of the decision team (warps 0-3 of the interval kernel)
+__device__ __forceinline__ void team_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
 struct MetroShared {
   double* d;      // current diagonal [N]
@@ -122,13 +136,19 @@ struct MetroShared {
   double* X;      // N x kmax
   double* Y;      // kmax x N (row-major)
   int* ired;      // >= 32 ints
+  int* qj;        // accepted site of each panel column [kmax]
+  double* qg;     // gamma of each panel column [kmax]
+  double* gam;    // speculative gamma of the sites of a search round [128]
+  volatile int* qn;    // panel columns published by the decision warp
+  volatile int* qdone; // decision phase of this panel finished
 };
 
 __device__ void metropolis_slice(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
                                  double& n_acc, int flags, long long log_base) {
   const int N = ch.N, kmax = ch.kmax;
-  const int ldx = N, ldy = N;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int ldp = panel_ld(N);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool log = (flags & HQ_F_LOG_RATIOS) && ch.ratios;
   // uniforms of this slice: site i consumes engine draws 2i+1, 2i+2 after the current state
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     const uint32_t x1 = minstd_mulmod(minstd_pow(2ull * i + 1), rng);
@@ -140,61 +160,296 @@ __device__ void metropolis_slice(const HqChain& ch, double* G, int ld, const Met
   rng = minstd_mulmod(minstd_pow(2ull * N), rng);
   __syncthreads();
   int k = 0, start = 0;
+  const int tid = threadIdx.x;
+  constexpr int kTeam = 128;  // warps 0-3 walk the decision chain, warps 4-7 fill panels
   while (true) {
-    // ---- find the first accepted site in [start, N) ----
-    int cand = INT_MAX;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-      if (i >= start) {
-        const double delta = sh.s[i] > 0 ? ch.delta_p : ch.delta_m;
-        const double a = 1.0 + (1.0 - sh.d[i]) * delta;
-        const double r = (a * a) / (1.0 + delta);
-        sh.rr[i] = r;
-        if (sh.u[i] < fmin(1.0, fabs(r)) && i < cand) cand = i;
+    // The decision team walks the chain of flips of this panel. For each accepted site j it
+    // computes the entries p > j of G's current column / row j (all that later decisions of
+    // this slice read) and the diagonal; the helper warps fill the entries p <= j of the
+    // same panel columns from a shared-memory queue, off the critical path.
+    if (tid == 0) { *sh.qn = 0; *sh.qdone = 0; }
+    __syncthreads();
+    if (tid < kTeam) {
+      int kk = 0, round = 0;
+      while (start < N && kk < kmax) {
+        // first accepted site >= start: 128 sites per round. accept iff u < min(1, |r|),
+        // r = a^2 / (1 + Delta), 1 + Delta = e^{-2 alpha s} > 0: u (1 + Delta) < a^2.
+        // gamma = Delta / a is formed speculatively by every accepting thread.
+        int j = -1;
+        for (int base = start; base < N; base += kTeam) {
+          const int i = base + tid;
+          bool acc = false;
+          if (i < N) {
+            const double delta = sh.s[i] > 0 ? ch.delta_p : ch.delta_m;
+            const double a = 1.0 + (1.0 - sh.d[i]) * delta;
+            if (log) sh.rr[i] = (a * a) / (1.0 + delta);
+            acc = sh.u[i] * (1.0 + delta) < a * a;
+            if (acc) sh.gam[tid] = delta / a;
+          }
+          const unsigned bal = __ballot_sync(0xffffffffu, acc);
+          int* wb = sh.ired + 8 + (round & 1) * 4;
+          if ((tid & 31) == 0) wb[tid >> 5] = bal ? (tid & ~31) + __ffs(bal) - 1 : kTeam;
+          team_sync();
+          ++round;
+          int first = kTeam;
+#pragma unroll
+          for (int w = 0; w < 4; ++w) first = min(first, wb[w]);
+          if (first < kTeam) { j = base + first; break; }
+        }
+        if (j < 0) { start = N; break; }
+        const double gamma = sh.gam[(j - start) % kTeam];  // written by the accepting thread of the round
+        for (int p = j + 1 + tid; p < N; p += kTeam) {
+          double c0 = G[p + (size_t)j * ld], c1 = 0.0, r0 = G[j + (size_t)p * ld], r1 = 0.0;
+          int m = 0;
+          for (; m + 1 < kk; m += 2) {
+            c0 = fma(sh.X[p + m * ldp], sh.Y[m * ldp + j], c0);
+            r0 = fma(sh.X[j + m * ldp], sh.Y[m * ldp + p], r0);
+            c1 = fma(sh.X[p + (m + 1) * ldp], sh.Y[(m + 1) * ldp + j], c1);
+            r1 = fma(sh.X[j + (m + 1) * ldp], sh.Y[(m + 1) * ldp + p], r1);
+          }
+          if (m < kk) {
+            c0 = fma(sh.X[p + m * ldp], sh.Y[m * ldp + j], c0);
+            r0 = fma(sh.X[j + m * ldp], sh.Y[m * ldp + p], r0);
+          }
+          const double xv = gamma * (c0 + c1);
+          const double yv = r0 + r1;
+          sh.X[p + kk * ldp] = xv;
+          sh.Y[kk * ldp + p] = yv;
+          sh.d[p] = fma(xv, yv, sh.d[p]);
+        }
+        if (tid == 0) {
+          sh.flip[j] = 1;
+          sh.qj[kk] = j;
+          sh.qg[kk] = gamma;
+        }
+        __threadfence_block();
+        team_sync();
+        if (tid == 0) *sh.qn = kk + 1;  // entries p > j of column kk are visible to everyone
+        n_acc += (tid == 0) ? 1.0 : 0.0;
+        ++kk;
+        start = j + 1;
+      }
+      if (tid == 0) {
+        sh.ired[0] = kk;
+        sh.ired[1] = start;
+        __threadfence_block();
+        *sh.qdone = 1;
+      }
+    } else {
+      // helpers: rows p <= j of every published panel column, in publication order
+      const int hid = tid - kTeam, nh = blockDim.x - kTeam;
+      int next = 0;
+      long long spins = 0;
+      while (true) {
+        int avail = *sh.qn;
+        if (next >= avail) {
+          if (*sh.qdone) {
+            __threadfence_block();
+            avail = *sh.qn;
+            if (next >= avail) break;
+          } else {
+            if (++spins > (1ll << 24)) { ch.acc[HQ_ACC_STATUS] = 2.0; break; }  // bounded wait
+            __nanosleep(64);
+            continue;
+          }
+        }
+        __threadfence_block();
+        const int j = sh.qj[next];
+        const double gamma = sh.qg[next];
+        for (int p = hid; p <= j; p += nh) {
+          double c0 = G[p + (size_t)j * ld], c1 = 0.0, r0 = G[j + (size_t)p * ld], r1 = 0.0;
+          int m = 0;
+          for (; m + 1 < next; m += 2) {
+            c0 = fma(sh.X[p + m * ldp], sh.Y[m * ldp + j], c0);
+            r0 = fma(sh.X[j + m * ldp], sh.Y[m * ldp + p], r0);
+            c1 = fma(sh.X[p + (m + 1) * ldp], sh.Y[(m + 1) * ldp + j], c1);
+            r1 = fma(sh.X[j + (m + 1) * ldp], sh.Y[(m + 1) * ldp + p], r1);
+          }
+          if (m < next) {
+            c0 = fma(sh.X[p + m * ldp], sh.Y[m * ldp + j], c0);
+            r0 = fma(sh.X[j + m * ldp], sh.Y[m * ldp + p], r0);
+          }
+          sh.X[p + next * ldp] = gamma * (c0 + c1);
+          sh.Y[next * ldp + p] = (r0 + r1) - (p == j ? 1.0 : 0.0);
+        }
+        ++next;
       }
     }
-    cand = __reduce_min_sync(0xffffffffu, cand);
-    if (lane == 0) sh.ired[warp] = cand;
     __syncthreads();
-    int first = INT_MAX;
-    for (int w = 0; w < nwarps; ++w) first = min(first, sh.ired[w]);
-    if (first == INT_MAX) break;
-    // ---- accept site j: append gamma*G[:,j] and (G[j,:] - e_j) to the panels ----
-    const int j = first;
-    const double delta = sh.s[j] > 0 ? ch.delta_p : ch.delta_m;
-    const double gamma = delta / (1.0 + (1.0 - sh.d[j]) * delta);
-    for (int p = threadIdx.x; p < N; p += blockDim.x) {
-      double col = G[p + (size_t)j * ld];
-      double row = G[j + (size_t)p * ld];
-      for (int m = 0; m < k; ++m) {
-        col = fma(sh.X[p + m * ldx], sh.Y[m * ldy + j], col);
-        row = fma(sh.X[j + m * ldx], sh.Y[m * ldy + p], row);
-      }
-      const double xv = gamma * col;
-      const double yv = row - (p == j ? 1.0 : 0.0);
-      sh.X[p + k * ldx] = xv;
-      sh.Y[k * ldy + p] = yv;
-      if (p != j) sh.d[p] = fma(xv, yv, sh.d[p]);
-      else sh.flip[p] = 1;
-    }
-    n_acc += 1.0;
-    ++k;
-    start = j + 1;
-    __syncthreads();
-    if (k == kmax) {
-      flush_panels(G, ld, N, sh.X, ldx, sh.Y, ldy, k);
+    k = sh.ired[0];
+    start = sh.ired[1];
+    if (k > 0 && (k == kmax || start >= N)) {
+      flush_panels(G, ld, N, sh.X, ldp, sh.Y, ldp, k);
       k = 0;
-      __syncthreads();
     }
-  }
-  if (k > 0) {
-    flush_panels(G, ld, N, sh.X, ldx, sh.Y, ldy, k);
+    __syncthreads();
+    if (start >= N) break;
   }
   // apply the flips of this slice and optionally log the visit-time ratios
   for (int i = threadIdx.x; i < N; i += blockDim.x) {
     if (sh.flip[i]) sh.s[i] = -sh.s[i];
-    if ((flags & HQ_F_LOG_RATIOS) && ch.ratios && log_base + i < ch.ratio_cap) ch.ratios[log_base + i] = sh.rr[i];
+    if (log && log_base + i < ch.ratio_cap) ch.ratios[log_base + i] = sh.rr[i];
   }
   __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------
+//  Register-panel Metropolis sweep of one slice (N <= blockDim.x, one site per thread).
+//
+//  Thread p owns site p: its uniform, field, current diagonal G_pp and its row of the
+//  delayed-update panels (X[p, :], Y[:, p]) live in registers. Sites of a slice are
+//  accepted in increasing order j_0 < j_1 < ..., so for a new flip j only the entries
+//  p > j of G's current column / row j can influence later decisions of the slice:
+//      col_p = G0[p, j] + sum_m X[p, m] Y[m, j],  row_p = G0[j, p] + sum_m X[j, m] Y[m, p]
+//  with Y[m, j] and X[j, m] (j > j_m) published by thread j in shared memory. The entries
+//  p <= j_m are filled just before the panel is flushed into G0 with DMMA.
+// ---------------------------------------------------------------------------------
+template <int KMAX>
+__device__ void metropolis_slice_reg(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
+                                     double& n_acc, int flags, long long log_base) {
+  const int N = ch.N;
+  const int kmax = ch.kmax < KMAX ? ch.kmax : KMAX;
+  const int ldp = panel_ld(N);
+  const int p = threadIdx.x;
+  const int lane = p & 31, warp = p >> 5, nwarps = blockDim.x >> 5;
+  const bool owner = p < N;
+  const bool log = (flags & HQ_F_LOG_RATIOS) && ch.ratios;
+  double u = 0.0, d = 0.0, dlt = 0.0, rr = 0.0;
+  bool flipped = false;
+  if (owner) {
+    const uint32_t x1 = minstd_mulmod(minstd_pow(2ull * p + 1), rng);
+    const uint32_t x2 = minstd_mulmod(kMinstdA, x1);
+    u = canonical_from_pair(x1, x2);
+    d = G[p + (size_t)p * ld];
+    dlt = sh.s[p] > 0 ? ch.delta_p : ch.delta_m;
+  }
+  rng = minstd_mulmod(minstd_pow(2ull * N), rng);
+  double Xr[KMAX], Yr[KMAX];
+#pragma unroll
+  for (int m = 0; m < KMAX; ++m) { Xr[m] = 0.0; Yr[m] = 0.0; }
+  int k = 0, start = 0, parity = 0;
+  while (true) {
+    // ---- first accepted site >= start: accept iff u (1 + Delta) < a^2 (u < min(1, |r|)) ----
+    int cand = INT_MAX;
+    if (owner && p >= start) {
+      const double a = 1.0 + (1.0 - d) * dlt;
+      if (log) rr = (a * a) / (1.0 + dlt);
+      if (u * (1.0 + dlt) < a * a) {
+        cand = p;
+        sh.gam[p] = dlt / a;  // gamma of this site, used only if it is the first
+      }
+    }
+    cand = __reduce_min_sync(0xffffffffu, cand);
+    int* wb = sh.ired + 8 + parity * 16;
+    parity ^= 1;
+    if (lane == 0) wb[warp] = cand;
+    __syncthreads();
+    int j = INT_MAX;
+    for (int w = 0; w < nwarps; ++w) j = min(j, wb[w]);
+    if (j == INT_MAX) break;
+    const double gamma = sh.gam[j];
+    // ---- append column k: entries p > j (later decisions read only those) ----
+    if (owner && p > j) {
+      double c0 = G[p + (size_t)j * ld], c1 = 0.0, r0 = G[j + (size_t)p * ld], r1 = 0.0;
+#pragma unroll
+      for (int m = 0; m < KMAX; m += 2) {
+        if (m < k) {
+          c0 = fma(Xr[m], sh.Y[m * ldp + j], c0);
+          r0 = fma(sh.X[j + m * ldp], Yr[m], r0);
+        }
+        if (m + 1 < k) {
+          c1 = fma(Xr[m + 1], sh.Y[(m + 1) * ldp + j], c1);
+          r1 = fma(sh.X[j + (m + 1) * ldp], Yr[m + 1], r1);
+        }
+      }
+      const double xv = gamma * (c0 + c1), yv = r0 + r1;
+#pragma unroll
+      for (int m = 0; m < KMAX; ++m)
+        if (m == k) { Xr[m] = xv; Yr[m] = yv; }
+      sh.X[p + k * ldp] = xv;
+      sh.Y[k * ldp + p] = yv;
+      d = fma(xv, yv, d);
+    }
+    if (p == j) flipped = true;
+    if (p == 0) { sh.qj[k] = j; sh.qg[k] = gamma; }
+    n_acc += (p == 0) ? 1.0 : 0.0;
+    ++k;
+    start = j + 1;
+    __syncthreads();
+    if (k == kmax || start >= N) {
+      // ---- fill the entries p <= j_m of the panel, then flush G0 += X Y ----
+      if (owner) {
+#pragma unroll
+        for (int m = 0; m < KMAX; ++m) {
+          if (m < k) {
+            const int jm = sh.qj[m];
+            if (p <= jm) {
+              double c = G[p + (size_t)jm * ld], r = G[jm + (size_t)p * ld];
+#pragma unroll
+              for (int m2 = 0; m2 < KMAX; ++m2)
+                if (m2 < m) {
+                  c = fma(Xr[m2], sh.Y[m2 * ldp + jm], c);
+                  r = fma(sh.X[jm + m2 * ldp], Yr[m2], r);
+                }
+              Xr[m] = sh.qg[m] * c;
+              Yr[m] = r - (p == jm ? 1.0 : 0.0);
+              sh.X[p + m * ldp] = Xr[m];
+              sh.Y[m * ldp + p] = Yr[m];
+            }
+          }
+        }
+      }
+      __syncthreads();
+      flush_panels(G, ld, N, sh.X, ldp, sh.Y, ldp, k);
+      k = 0;
+      __syncthreads();
+      if (owner) d = G[p + (size_t)p * ld];
+      if (start >= N) break;
+    }
+  }
+  if (k > 0) {
+    // a slice that ended on a round without acceptance: fill and flush the open panel
+    if (owner) {
+#pragma unroll
+      for (int m = 0; m < KMAX; ++m) {
+        if (m < k) {
+          const int jm = sh.qj[m];
+          if (p <= jm) {
+            double c = G[p + (size_t)jm * ld], r = G[jm + (size_t)p * ld];
+#pragma unroll
+            for (int m2 = 0; m2 < KMAX; ++m2)
+              if (m2 < m) {
+                c = fma(Xr[m2], sh.Y[m2 * ldp + jm], c);
+                r = fma(sh.X[jm + m2 * ldp], Yr[m2], r);
+              }
+            Xr[m] = sh.qg[m] * c;
+            Yr[m] = r - (p == jm ? 1.0 : 0.0);
+            sh.X[p + m * ldp] = Xr[m];
+            sh.Y[m * ldp + p] = Yr[m];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    flush_panels(G, ld, N, sh.X, ldp, sh.Y, ldp, k);
+    __syncthreads();
+  }
+  if (owner) {
+    if (flipped) sh.s[p] = -sh.s[p];
+    if (log && log_base + p < ch.ratio_cap) ch.ratios[log_base + p] = rr;
+  }
+  __syncthreads();
+}
+
+// picks the register-panel sweep when every site has its own thread
+__device__ void metropolis_dispatch(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
+                                    double& n_acc, int flags, long long log_base) {
+  if (ch.N <= (int)blockDim.x) {
+    if (ch.kmax <= 8) metropolis_slice_reg<8>(ch, G, ld, sh, rng, n_acc, flags, log_base);
+    else metropolis_slice_reg<16>(ch, G, ld, sh, rng, n_acc, flags, log_base);
+  } else {
+    metropolis_slice(ch, G, ld, sh, rng, n_acc, flags, log_base);
+  }
 }
 
 // ---------------------------------------------------------------------------------
@@ -207,16 +462,14 @@ __device__ void wrap_slice(const HqChain& ch, double* G, int ld, const int8_t* s
   if (dir == HQ_UP) {
     apply_expk(ch, G, ld, 0, false, stage);
     apply_expk(ch, G, ld, 1, true, stage);
-    for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-      const int i = idx % N, j = idx / N;
+    HQ_FOR_EACH_ELEM(N, i, j) {
       const double fi = s[i] > 0 ? ch.ev_p : ch.ev_m;
       const double fj = s[j] > 0 ? ch.ev_m : ch.ev_p;
       G[i + (size_t)j * ld] *= fi * fj;
     }
     __syncthreads();
   } else {
-    for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-      const int i = idx % N, j = idx / N;
+    HQ_FOR_EACH_ELEM(N, i, j) {
       const double fi = s[i] > 0 ? ch.ev_m : ch.ev_p;
       const double fj = s[j] > 0 ? ch.ev_p : ch.ev_m;
       G[i + (size_t)j * ld] *= fi * fj;
@@ -238,12 +491,12 @@ __device__ __host__ inline void interval_range(int nt, int pace, int n_stab, int
 // ---------------------------------------------------------------------------------
 //  k_interval: the update (or no-update) slices of one stabilisation interval.
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(HQ_THREADS, 1)
+__global__ void __launch_bounds__(HQ_INT_THREADS, 1)
 k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int flags, int resident) {
   extern __shared__ __align__(16) double smem[];
   __shared__ HqChain ch;
-  __shared__ double red[32];
-  __shared__ int ired[32];
+  __shared__ double red[96];
+  __shared__ int ired[64];
   const int c = blockIdx.x;
   if (c >= nchains) return;
   if (threadIdx.x == 0) ch = chains[c];
@@ -266,19 +519,28 @@ k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int 
     G = ch.G;
     ld = N;
   }
-  const size_t panels = (size_t)N * ch.kmax * 2;
+  const size_t panels = (size_t)panel_ld(N) * ch.kmax * 2;
   const size_t stage_n = (size_t)8 * (((N + 15) & ~15) + 4);
   double* work = p;
   p += panels > stage_n ? panels : stage_n;
   MetroShared sh;
   sh.X = work;
-  sh.Y = work + (size_t)N * ch.kmax;
+  sh.Y = work + (size_t)panel_ld(N) * ch.kmax;
   sh.d = p; p += N;
   sh.u = p; p += N;
   sh.rr = p; p += N;
   sh.s = reinterpret_cast<int8_t*>(p);
   sh.flip = sh.s + N;
   sh.ired = ired;
+  __shared__ int qj_s[64];
+  __shared__ double qg_s[64];
+  __shared__ double gam_s[HQ_INT_THREADS];
+  sh.gam = gam_s;
+  __shared__ int qn_s, qdone_s;
+  sh.qj = qj_s;
+  sh.qg = qg_s;
+  sh.qn = &qn_s;
+  sh.qdone = &qdone_s;
   uint32_t rng = *ch.rng;
   double n_acc = 0.0, n_prop = 0.0;
   long long log_base = (flags & HQ_F_LOG_RATIOS) && ch.ratio_count ? *ch.ratio_count : 0;
@@ -292,11 +554,11 @@ k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int 
     __syncthreads();
     if (dir == HQ_UP) {
       wrap_slice(ch, G, ld, sh.s, HQ_UP, work);
-      metropolis_slice(ch, G, ld, sh, rng, n_acc, flags, log_base);
+      metropolis_dispatch(ch, G, ld, sh, rng, n_acc, flags, log_base);
       n_prop += N;
       log_base += N;
     } else if (dir == HQ_DOWN) {
-      metropolis_slice(ch, G, ld, sh, rng, n_acc, flags, log_base);
+      metropolis_dispatch(ch, G, ld, sh, rng, n_acc, flags, log_base);
       n_prop += N;
       log_base += N;
       wrap_slice(ch, G, ld, sh.s, HQ_DOWN, work);
@@ -330,7 +592,7 @@ k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int 
 //  init: the right stack at initialisation (src/dqmc_core.cpp:67-87) is the down
 //  direction without updates.
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(HQ_THREADS, 1)
+__global__ void __launch_bounds__(HQ_INT_THREADS, 1)
 k_bchain(const HqChain* __restrict__ chains, int nchains, int dir, int b, int resident) {
   extern __shared__ __align__(16) double smem[];
   __shared__ HqChain ch;
@@ -353,10 +615,7 @@ k_bchain(const HqChain* __restrict__ chains, int nchains, int dir, int b, int re
   const size_t NN = (size_t)N * N;
   const double* U = top >= 0 ? ch.stackU + ((size_t)side * ch.n_stab + top) * NN : nullptr;
   const double* D = top >= 0 ? ch.stackD + ((size_t)side * ch.n_stab + top) * N : nullptr;
-  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-    const int i = idx % N, j = idx / N;
-    X[i + (size_t)j * ld] = U ? U[idx] * D[j] : (i == j ? 1.0 : 0.0);
-  }
+  HQ_FOR_EACH_ELEM(N, i, j) X[i + (size_t)j * ld] = U ? U[i + (size_t)j * N] * D[j] : (i == j ? 1.0 : 0.0);
   __syncthreads();
   const int nsl = t_hi - t_lo + 1;
   for (int step = 0; step < nsl; ++step) {
@@ -378,17 +637,69 @@ k_bchain(const HqChain* __restrict__ chains, int nchains, int dir, int b, int re
 }
 
 // ---------------------------------------------------------------------------------
-//  k_udt: X P = Q R (column-pivoted Householder QR, LAPACK dgeqp3/dlaqp2 order), then
+//  k_udt: X P = Q R (column-pivoted Householder QR in LAPACK dgeqp3/dlaqp2 order), then
 //  D = |diag R|, T = D^-1 R P^T, and Q formed in place (dorg2r order).
-//  Output: U -> stack entry, D -> stack entry, T -> W0.
+//  Output: U (= Q) and D into stack entry b of the pushing stack, T into W0.
+//  Warp 0 does the serial part of every step (pivot, column swap, reflector); all warps
+//  then update the trailing columns, four columns per warp at a time, and downdate the
+//  partial column norms.
 // ---------------------------------------------------------------------------------
+__device__ inline void householder_trailing(double* A, int ld, int N, int i, double ti, double* vn1, double* vn2,
+                                            bool downdate, bool v_implicit_one) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const double tol3z = 1.4901161193847656e-08;  // sqrt(eps)
+  for (int j0 = i + 1 + warp * 4; j0 < N; j0 += nwarps * 4) {
+    double w[4] = {0.0, 0.0, 0.0, 0.0};
+    if (ti != 0.0) {
+      for (int r = i + lane; r < N; r += 32) {
+        const double v = (r == i && v_implicit_one) ? 1.0 : A[r + (size_t)i * ld];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (j0 + q < N) w[q] = fma(v, A[r + (size_t)(j0 + q) * ld], w[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) w[q] = warp_sum(w[q]) * ti;
+      for (int r = i + lane; r < N; r += 32) {
+        const double v = (r == i && v_implicit_one) ? 1.0 : A[r + (size_t)i * ld];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (j0 + q < N) A[r + (size_t)(j0 + q) * ld] = fma(-w[q], v, A[r + (size_t)(j0 + q) * ld]);
+      }
+    }
+    if (!downdate) continue;
+    __syncwarp();
+    // partial norm downdate of the (up to) four columns, lane q for column j0 + q
+    bool need = false;
+    {
+      const int j = j0 + lane;
+      if (lane < 4 && j < N) {
+        const double nv1 = vn1[j];
+        if (nv1 != 0.0) {
+          double temp = fabs(A[i + (size_t)j * ld]) / nv1;
+          temp = fmax(1.0 - temp * temp, 0.0);
+          const double r2 = nv1 / vn2[j];
+          if (temp * r2 * r2 <= tol3z) need = true;
+          else vn1[j] = nv1 * sqrt(temp);
+        }
+      }
+    }
+    unsigned nb = __ballot_sync(0xffffffffu, need);
+    while (nb) {
+      const int j = j0 + __ffs(nb) - 1;
+      nb &= nb - 1;
+      double s2 = 0.0;
+      for (int r = i + 1 + lane; r < N; r += 32) { const double v = A[r + (size_t)j * ld]; s2 = fma(v, v, s2); }
+      s2 = warp_sum(s2);
+      if (lane == 0) { vn1[j] = sqrt(s2); vn2[j] = vn1[j]; }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(HQ_THREADS, 1)
-k_udt(const HqChain* __restrict__ chains, int nchains, int side, int entry_from_len, int b, int resident) {
+k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int b, int resident) {
   extern __shared__ __align__(16) double smem[];
   __shared__ HqChain ch;
-  __shared__ double red[32];
-  __shared__ int piv_s;
-  __shared__ double tau_s, beta_s;
+  __shared__ double tau_s;
   const int c = blockIdx.x;
   if (c >= nchains) return;
   if (threadIdx.x == 0) ch = chains[c];
@@ -408,7 +719,6 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int entry_from_
   int* jpvt = reinterpret_cast<int*>(p);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   __syncthreads();
-  // column norms
   for (int j = warp; j < N; j += nwarps) {
     double s2 = 0.0;
     for (int i = lane; i < N; i += 32) { const double v = A[i + (size_t)j * ld]; s2 = fma(v, v, s2); }
@@ -416,10 +726,9 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int entry_from_
     if (lane == 0) { vn1[j] = sqrt(s2); vn2[j] = vn1[j]; jpvt[j] = j; }
   }
   __syncthreads();
-  const double tol3z = sqrt(2.220446049250313e-16);
   for (int i = 0; i < N; ++i) {
-    // pivot: argmax vn1[i:N] (first maximum, as idamax)
     if (warp == 0) {
+      // pivot: first maximum of vn1[i:N] (idamax)
       double best = -1.0;
       int bi = i;
       for (int j = i + lane; j < N; j += 32) {
@@ -432,79 +741,40 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int entry_from_
         const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
         if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
       }
-      if (lane == 0) piv_s = bi;
-    }
-    __syncthreads();
-    const int pv = piv_s;
-    if (pv != i) {
-      for (int r = threadIdx.x; r < N; r += blockDim.x) {
-        const double t0 = A[r + (size_t)pv * ld];
-        A[r + (size_t)pv * ld] = A[r + (size_t)i * ld];
-        A[r + (size_t)i * ld] = t0;
-      }
-      if (threadIdx.x == 0) {
-        const int tj = jpvt[pv]; jpvt[pv] = jpvt[i]; jpvt[i] = tj;
-        vn1[pv] = vn1[i];
-        vn2[pv] = vn2[i];
-      }
-    }
-    __syncthreads();
-    // Householder reflector of A[i:N, i] (dlarfg)
-    double xs = 0.0;
-    for (int r = i + 1 + threadIdx.x; r < N; r += blockDim.x) { const double v = A[r + (size_t)i * ld]; xs = fma(v, v, xs); }
-    xs = block_sum(xs, red);
-    if (threadIdx.x == 0) {
-      const double alpha = A[i + (size_t)i * ld];
-      const double xnorm = sqrt(xs);
-      if (xnorm == 0.0) { tau_s = 0.0; beta_s = alpha; }
-      else {
-        const double beta = -copysign(hypot(alpha, xnorm), alpha);
-        tau_s = (beta - alpha) / beta;
-        beta_s = beta;
-        wv[0] = 1.0 / (alpha - beta);
-      }
-    }
-    __syncthreads();
-    const double ti = tau_s;
-    if (ti != 0.0) {
-      const double sc = wv[0];
-      for (int r = i + 1 + threadIdx.x; r < N; r += blockDim.x) A[r + (size_t)i * ld] *= sc;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) { A[i + (size_t)i * ld] = beta_s; tau[i] = ti; }
-    // apply H = I - tau v v^T to A[i:N, i+1:N], v = [1; A[i+1:N, i]]; one warp per column
-    if (ti != 0.0) {
-      for (int j = i + 1 + warp; j < N; j += nwarps) {
-        double w = (lane == 0) ? A[i + (size_t)j * ld] : 0.0;
-        for (int r = i + 1 + lane; r < N; r += 32) w = fma(A[r + (size_t)i * ld], A[r + (size_t)j * ld], w);
-        w = warp_sum(w) * ti;
-        if (lane == 0) A[i + (size_t)j * ld] -= w;
-        for (int r = i + 1 + lane; r < N; r += 32) A[r + (size_t)j * ld] = fma(-w, A[r + (size_t)i * ld], A[r + (size_t)j * ld]);
-      }
-    }
-    __syncthreads();
-    // partial column norm downdate (dlaqp2)
-    for (int j = i + 1 + warp; j < N; j += nwarps) {
-      double nv1 = vn1[j];
-      if (nv1 != 0.0) {
-        double temp = fabs(A[i + (size_t)j * ld]) / nv1;
-        temp = 1.0 - temp * temp;
-        temp = fmax(temp, 0.0);
-        const double r2 = nv1 / vn2[j];
-        const double temp2 = temp * r2 * r2;
-        if (temp2 <= tol3z) {
-          double s2 = 0.0;
-          for (int r = i + 1 + lane; r < N; r += 32) { const double v = A[r + (size_t)j * ld]; s2 = fma(v, v, s2); }
-          s2 = warp_sum(s2);
-          if (lane == 0) { vn1[j] = sqrt(s2); vn2[j] = vn1[j]; }
-        } else {
-          if (lane == 0) vn1[j] = nv1 * sqrt(temp);
+      if (bi != i) {
+        for (int r = lane; r < N; r += 32) {
+          const double t0 = A[r + (size_t)bi * ld];
+          A[r + (size_t)bi * ld] = A[r + (size_t)i * ld];
+          A[r + (size_t)i * ld] = t0;
+        }
+        if (lane == 0) {
+          const int tj = jpvt[bi]; jpvt[bi] = jpvt[i]; jpvt[i] = tj;
+          vn1[bi] = vn1[i];
+          vn2[bi] = vn2[i];
         }
       }
+      __syncwarp();
+      // reflector of A[i:N, i] (dlarfg)
+      double xs = 0.0;
+      for (int r = i + 1 + lane; r < N; r += 32) { const double v = A[r + (size_t)i * ld]; xs = fma(v, v, xs); }
+      xs = warp_sum(xs);
+      const double alpha = A[i + (size_t)i * ld];
+      double ti = 0.0, beta = alpha;
+      if (xs > 0.0) {
+        beta = -copysign(hypot(alpha, sqrt(xs)), alpha);
+        ti = (beta - alpha) / beta;
+        const double sc = 1.0 / (alpha - beta);
+        for (int r = i + 1 + lane; r < N; r += 32) A[r + (size_t)i * ld] *= sc;
+      }
+      __syncwarp();
+      if (lane == 0) { A[i + (size_t)i * ld] = beta; tau[i] = ti; tau_s = ti; }
     }
     __syncthreads();
+    // apply H(i) = I - tau v v^T to A[i:N, i+1:N] (v_i = 1) and downdate the norms
+    householder_trailing(A, ld, N, i, tau_s, vn1, vn2, true, true);
+    __syncthreads();
   }
-  // D and T = D^-1 R P^T (T[:, jpvt[c]] = row-scaled R[:, c])
+  // D = |diag R| and T = D^-1 R P^T  (T[:, jpvt[c]] = row-scaled R[:, c])
   const size_t NN = (size_t)N * N;
   double* Dout = ch.stackD + ((size_t)side * ch.n_stab + entry) * N;
   double* T = ch.W0;
@@ -514,25 +784,16 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int entry_from_
     wv[r] = dr;
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-    const int r = idx % N, cc = idx / N;
+  HQ_FOR_EACH_ELEM(N, r, cc) {
     const double v = (r <= cc) ? A[r + (size_t)cc * ld] / wv[r] : 0.0;
     T[r + (size_t)jpvt[cc] * N] = (wv[r] != 0.0) ? v : (r == cc ? 1.0 : 0.0);
   }
   __syncthreads();
-  // form Q in place from the reflectors (dorg2r): for i = N-1 .. 0
+  // form Q in place from the reflectors (dorg2r): i = N-1 .. 0
   for (int i = N - 1; i >= 0; --i) {
     const double ti = tau[i];
     if (i < N - 1) {
-      if (threadIdx.x == 0) A[i + (size_t)i * ld] = 1.0;
-      __syncthreads();
-      // apply H(i) to A[i:N, i+1:N]
-      for (int j = i + 1 + warp; j < N; j += nwarps) {
-        double w = 0.0;
-        for (int r = i + lane; r < N; r += 32) w = fma(A[r + (size_t)i * ld], A[r + (size_t)j * ld], w);
-        w = warp_sum(w) * ti;
-        for (int r = i + lane; r < N; r += 32) A[r + (size_t)j * ld] = fma(-w, A[r + (size_t)i * ld], A[r + (size_t)j * ld]);
-      }
+      householder_trailing(A, ld, N, i, ti, vn1, vn2, false, true);
       __syncthreads();
       for (int r = i + 1 + threadIdx.x; r < N; r += blockDim.x) A[r + (size_t)i * ld] *= -ti;
     }
@@ -546,14 +807,16 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int entry_from_
 
 // ---------------------------------------------------------------------------------
 //  k_invert: in-place Gauss-Jordan inverse with partial (row) pivoting of the N x N
-//  matrix at `which` (0: W1, 1: W2, 2: W3, 3: W5). Failure (zero pivot / non-finite) sets acc[STATUS].
+//  matrix at `which` (0: W1, 1: W2, 2: W3, 3: W5). Two barriers per pivot: warp 0 finds
+//  the pivot and stages the scaled pivot row (prow) and the old row k (krow); then every
+//  warp eliminates its own rows. The row interchanges are undone as one column gather on
+//  the way out. Failure (zero pivot / non-finite) sets acc[STATUS].
 // ---------------------------------------------------------------------------------
 __global__ void __launch_bounds__(HQ_THREADS, 1)
 k_invert(const HqChain* __restrict__ chains, int nchains, int b, int which, int resident) {
   extern __shared__ __align__(16) double smem[];
   __shared__ HqChain ch;
   __shared__ int piv_s;
-  __shared__ double pinv_s;
   const int c = blockIdx.x;
   if (c >= nchains) return;
   if (threadIdx.x == 0) ch = chains[c];
@@ -566,9 +829,11 @@ k_invert(const HqChain* __restrict__ chains, int nchains, int b, int which, int 
   double* p = smem;
   if (resident) { A = p; ld = smem_ld(N); p += (size_t)N * ld; copy_mat(A, ld, src, N, N); }
   else { A = src; ld = N; }
-  double* colk = p; p += N;
+  double* prow = p; p += N;
+  double* krow = p; p += N;
   int* perm = reinterpret_cast<int*>(p);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int* gidx = perm + N;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   __syncthreads();
   for (int k = 0; k < N; ++k) {
     if (warp == 0) {
@@ -584,60 +849,60 @@ k_invert(const HqChain* __restrict__ chains, int nchains, int b, int which, int 
         const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
         if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
       }
+      const double pval = A[bi + (size_t)k * ld];
+      const bool ok = (best > 0.0) && isfinite(best);
+      const double pinv = ok ? 1.0 / pval : 0.0;
+      for (int j = lane; j < N; j += 32) {
+        krow[j] = A[k + (size_t)j * ld];
+        prow[j] = (j == k ? 1.0 : A[bi + (size_t)j * ld]) * pinv;
+      }
       if (lane == 0) {
-        piv_s = bi;
         perm[k] = bi;
-        if (!(best > 0.0) || !isfinite(best)) ch.acc[HQ_ACC_STATUS] = 1.0;
+        piv_s = bi;
+        if (!ok) ch.acc[HQ_ACC_STATUS] = 1.0;
       }
     }
     __syncthreads();
     const int pr = piv_s;
-    if (pr != k) {
-      for (int j = threadIdx.x; j < N; j += blockDim.x) {
-        const double t0 = A[k + (size_t)j * ld];
-        A[k + (size_t)j * ld] = A[pr + (size_t)j * ld];
-        A[pr + (size_t)j * ld] = t0;
+    for (int r = warp; r < N; r += nwarps) {
+      if (r == k) {
+        for (int j = lane; j < N; j += 32) A[k + (size_t)j * ld] = prow[j];
+        continue;
       }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const double pv = A[k + (size_t)k * ld];
-      pinv_s = (pv != 0.0) ? 1.0 / pv : 0.0;
-    }
-    __syncthreads();
-    const double pinv = pinv_s;
-    // save column k, scale pivot row, with A[k,k] := 1 before scaling
-    for (int r = threadIdx.x; r < N; r += blockDim.x) colk[r] = A[r + (size_t)k * ld];
-    __syncthreads();
-    for (int j = threadIdx.x; j < N; j += blockDim.x) {
-      const double v = (j == k) ? 1.0 : A[k + (size_t)j * ld];
-      A[k + (size_t)j * ld] = v * pinv;
-    }
-    __syncthreads();
-    // eliminate column k from every other row
-    for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-      const int r = idx % N, j = idx / N;
-      if (r != k) {
-        const double f = colk[r];
-        const double base = (j == k) ? 0.0 : A[r + (size_t)j * ld];
-        A[r + (size_t)j * ld] = fma(-f, A[k + (size_t)j * ld], base);
+      const bool from_k = (r == pr);
+      const double f = from_k ? krow[k] : A[r + (size_t)k * ld];
+      __syncwarp();
+      for (int j = lane; j < N; j += 32) {
+        const double s0 = from_k ? krow[j] : A[r + (size_t)j * ld];
+        A[r + (size_t)j * ld] = fma(-f, prow[j], (j == k) ? 0.0 : s0);
       }
     }
     __syncthreads();
   }
-  // undo the row interchanges as column interchanges, in reverse order
-  for (int k = N - 1; k >= 0; --k) {
-    const int pr = perm[k];
-    if (pr != k) {
-      for (int r = threadIdx.x; r < N; r += blockDim.x) {
-        const double t0 = A[r + (size_t)k * ld];
-        A[r + (size_t)k * ld] = A[r + (size_t)pr * ld];
-        A[r + (size_t)pr * ld] = t0;
-      }
+  // undo the row interchanges as column interchanges in reverse order: column j of the
+  // inverse is column gidx[j] of A
+  if (threadIdx.x == 0) {
+    for (int j = 0; j < N; ++j) gidx[j] = j;
+    for (int k = N - 1; k >= 0; --k) {
+      const int t0 = gidx[k]; gidx[k] = gidx[perm[k]]; gidx[perm[k]] = t0;
     }
-    __syncthreads();
   }
-  if (resident) copy_mat(src, N, A, ld, N);
+  __syncthreads();
+  if (resident) {
+    HQ_FOR_EACH_ELEM(N, i, j) src[i + (size_t)j * N] = A[i + (size_t)gidx[j] * ld];
+  } else {
+    // in global memory: apply the interchanges one by one
+    for (int k = N - 1; k >= 0; --k) {
+      const int q = perm[k];
+      if (q != k)
+        for (int r = threadIdx.x; r < N; r += blockDim.x) {
+          const double t0 = A[r + (size_t)k * ld];
+          A[r + (size_t)k * ld] = A[r + (size_t)q * ld];
+          A[r + (size_t)q * ld] = t0;
+        }
+      __syncthreads();
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------------
@@ -655,10 +920,42 @@ __device__ __forceinline__ double vscale(const double* v, int mode, int i) {
 
 constexpr int GBM = 64, GBN = 64, GBK = 16, GLD = 68;
 
+// 8-byte asynchronous global -> shared copy; zero-fills (reads 0 bytes of `src`, which
+// the callers keep pointing at the operand's base) when `valid` is false
+__device__ __forceinline__ void cp_async_8(double* dst, const double* src, bool valid) {
+  const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  const int nbytes = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(src), "r"(nbytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND)); }
+
+__device__ __forceinline__ void gemm_load_chunk(const HqGemmJob& J, int m0, int n0, int k0, double* sA, double* sB) {
+  // op(A) tile rows m0..m0+63, cols k0..k0+15 -> sA[k][m]; op(B) rows k0..k0+15, cols n0..n0+63 -> sB[k][n]
+  for (int idx = threadIdx.x; idx < GBM * GBK; idx += blockDim.x) {
+    int m, k;
+    if (!J.ta) { m = idx % GBM; k = idx / GBM; } else { k = idx % GBK; m = idx / GBK; }
+    const int gm = m0 + m, gk = k0 + k;
+    const bool ok = gm < J.M && gk < J.K;
+    const double* src = ok ? (!J.ta ? J.A + gm + (size_t)gk * J.lda : J.A + gk + (size_t)gm * J.lda) : J.A;
+    cp_async_8(sA + k * GLD + m, src, ok);
+  }
+  for (int idx = threadIdx.x; idx < GBK * GBN; idx += blockDim.x) {
+    int k, n;
+    if (!J.tb) { k = idx % GBK; n = idx / GBK; } else { n = idx % GBN; k = idx / GBN; }
+    const int gk = k0 + k, gn = n0 + n;
+    const bool ok = gk < J.K && gn < J.Nc;
+    const double* src = ok ? (!J.tb ? J.B + gk + (size_t)gn * J.ldb : J.B + gn + (size_t)gk * J.ldb) : J.B;
+    cp_async_8(sB + k * GLD + n, src, ok);
+  }
+}
+
 __global__ void __launch_bounds__(128)
 k_gemm(const HqGemmJob* __restrict__ jobs, int njobs, int tiles_n) {
-  __shared__ __align__(16) double sA[GBK * GLD];
-  __shared__ __align__(16) double sB[GBK * GLD];
+  __shared__ __align__(16) double sA[2][GBK * GLD];
+  __shared__ __align__(16) double sB[2][GBK * GLD];
+  __shared__ double sK[2][GBK];
   __shared__ double red[32];
   const int jb = blockIdx.y;
   if (jb >= njobs) return;
@@ -675,46 +972,41 @@ k_gemm(const HqGemmJob* __restrict__ jobs, int njobs, int tiles_n) {
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = acc[a][b][2] = acc[a][b][3] = 0.0;
-  for (int k0 = 0; k0 < J.K; k0 += GBK) {
-    __syncthreads();
-    // op(A) tile: rows m0..m0+63, cols k0..k0+15 -> sA[k][m]
-    for (int idx = threadIdx.x; idx < GBM * GBK; idx += blockDim.x) {
-      int m, k;
-      if (!J.ta) { m = idx % GBM; k = idx / GBM; } else { k = idx % GBK; m = idx / GBK; }
-      const int gm = m0 + m, gk = k0 + k;
-      double v = 0.0;
-      if (gm < J.M && gk < J.K) {
-        v = !J.ta ? J.A[gm + (size_t)gk * J.lda] : J.A[gk + (size_t)gm * J.lda];
-        v *= vscale(J.ks, J.ks_mode, gk);
-      }
-      sA[k * GLD + m] = v;
+  const int nchunks = (J.K + GBK - 1) / GBK;
+  gemm_load_chunk(J, m0, n0, 0, sA[0], sB[0]);
+  if (threadIdx.x < GBK) sK[0][threadIdx.x] = (threadIdx.x < J.K) ? vscale(J.ks, J.ks_mode, threadIdx.x) : 0.0;
+  cp_async_commit();
+  for (int c = 0; c < nchunks; ++c) {
+    const int cur = c & 1;
+    if (c + 1 < nchunks) {
+      const int k1 = (c + 1) * GBK;
+      gemm_load_chunk(J, m0, n0, k1, sA[cur ^ 1], sB[cur ^ 1]);
+      if (threadIdx.x < GBK) sK[cur ^ 1][threadIdx.x] = (k1 + threadIdx.x < J.K) ? vscale(J.ks, J.ks_mode, k1 + threadIdx.x) : 0.0;
     }
-    // op(B) tile: rows k0..k0+15, cols n0..n0+63 -> sB[k][n]
-    for (int idx = threadIdx.x; idx < GBK * GBN; idx += blockDim.x) {
-      int k, n;
-      if (!J.tb) { k = idx % GBK; n = idx / GBK; } else { n = idx % GBN; k = idx / GBN; }
-      const int gk = k0 + k, gn = n0 + n;
-      double v = 0.0;
-      if (gk < J.K && gn < J.Nc) v = !J.tb ? J.B[gk + (size_t)gn * J.ldb] : J.B[gn + (size_t)gk * J.ldb];
-      sB[k * GLD + n] = v;
-    }
+    cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
+    const double* A_ = sA[cur];
+    const double* B_ = sB[cur];
 #pragma unroll
     for (int kk = 0; kk < GBK; kk += 4) {
       double a[2][2], bb[4];
+      const double kscale = sK[cur][kk + q];
 #pragma unroll
       for (int a_ = 0; a_ < 2; ++a_) {
-        a[a_][0] = sA[(kk + q) * GLD + wm + a_ * 16 + g];
-        a[a_][1] = sA[(kk + q) * GLD + wm + a_ * 16 + g + 8];
+        a[a_][0] = A_[(kk + q) * GLD + wm + a_ * 16 + g] * kscale;
+        a[a_][1] = A_[(kk + q) * GLD + wm + a_ * 16 + g + 8] * kscale;
       }
 #pragma unroll
-      for (int b_ = 0; b_ < 4; ++b_) bb[b_] = sB[(kk + q) * GLD + wn + b_ * 8 + g];
+      for (int b_ = 0; b_ < 4; ++b_) bb[b_] = B_[(kk + q) * GLD + wn + b_ * 8 + g];
 #pragma unroll
       for (int a_ = 0; a_ < 2; ++a_)
 #pragma unroll
         for (int b_ = 0; b_ < 4; ++b_) dmma_16x8x4(acc[a_][b_], a[a_][0], a[a_][1], bb[b_]);
     }
+    __syncthreads();
   }
+  cp_async_wait<0>();
   // epilogue
   double emax = -INFINITY;
 #pragma unroll
@@ -747,7 +1039,7 @@ k_gemm(const HqGemmJob* __restrict__ jobs, int njobs, int tiles_n) {
 __global__ void __launch_bounds__(HQ_THREADS)
 k_measure(const HqChain* __restrict__ chains, int nchains, int dir, int b, int flags) {
   __shared__ HqChain ch;
-  __shared__ double red[32];
+  __shared__ double red[96];
   const int c = blockIdx.x;
   if (c >= nchains) return;
   if (threadIdx.x == 0) ch = chains[c];
@@ -769,7 +1061,7 @@ k_measure(const HqChain* __restrict__ chains, int nchains, int dir, int b, int f
 //  CTA (blockIdx.y = 0: G(t,t), 1: G(t,0), 2: G(0,t)), except for the last slice which
 //  is rebuilt by the boundary step, and stores the per-slice results.
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(HQ_THREADS, 1)
+__global__ void __launch_bounds__(HQ_INT_THREADS, 1)
 k_dyn_slices(const HqChain* __restrict__ chains, int nchains, int b, int flags, int resident) {
   extern __shared__ __align__(16) double smem[];
   __shared__ HqChain ch;
@@ -965,7 +1257,7 @@ __device__ void adj_accum(const HqChain& ch, const double* G, int ld, const int8
   }
 }
 
-__global__ void __launch_bounds__(HQ_THREADS, 1)
+__global__ void __launch_bounds__(HQ_INT_THREADS, 1)
 k_adj_interval(const HqChain* __restrict__ chains, int nchains, int b, int resident) {
   extern __shared__ __align__(16) double smem[];
   __shared__ HqChain ch;
@@ -1045,7 +1337,7 @@ cudaError_t prepare_kernels(int Nmax, int kmax, bool resident) {
   if ((e = set_smem((const void*)k_interval, smem_interval_bytes(Nmax, kmax, resident))) != cudaSuccess) return e;
   if ((e = set_smem((const void*)k_bchain, mat_stage)) != cudaSuccess) return e;
   if ((e = set_smem((const void*)k_udt, smem_matrix_bytes(Nmax, resident, 5 * Nmax + 64))) != cudaSuccess) return e;
-  if ((e = set_smem((const void*)k_invert, smem_matrix_bytes(Nmax, resident, 2 * Nmax + 64))) != cudaSuccess) return e;
+  if ((e = set_smem((const void*)k_invert, smem_matrix_bytes(Nmax, resident, 3 * Nmax + 64))) != cudaSuccess) return e;
   if ((e = set_smem((const void*)k_dyn_slices, mat_stage)) != cudaSuccess) return e;
   if ((e = set_smem((const void*)k_adj_interval, mat_stage)) != cudaSuccess) return e;
   return cudaSuccess;
@@ -1054,12 +1346,12 @@ cudaError_t prepare_kernels(int Nmax, int kmax, bool resident) {
 cudaError_t launch_interval(const HqChain* chains, int n, int dir, int b, int flags, int Nmax, int kmax, bool resident,
                             cudaStream_t st) {
   const size_t bytes = smem_interval_bytes(Nmax, kmax, resident);
-  k_interval<<<n, HQ_THREADS, bytes, st>>>(chains, n, dir, b, flags, resident ? 1 : 0);
+  k_interval<<<n, HQ_INT_THREADS, bytes, st>>>(chains, n, dir, b, flags, resident ? 1 : 0);
   return cudaGetLastError();
 }
 cudaError_t launch_bchain(const HqChain* chains, int n, int dir, int b, int Nmax, bool resident, cudaStream_t st) {
   const size_t bytes = smem_matrix_bytes(Nmax, resident, 8 * (((Nmax + 15) & ~15) + 4) + 64);
-  k_bchain<<<n, HQ_THREADS, bytes, st>>>(chains, n, dir, b, resident ? 1 : 0);
+  k_bchain<<<n, HQ_INT_THREADS, bytes, st>>>(chains, n, dir, b, resident ? 1 : 0);
   return cudaGetLastError();
 }
 cudaError_t launch_udt(const HqChain* chains, int n, int side, int b, int Nmax, bool resident, cudaStream_t st) {
@@ -1068,7 +1360,7 @@ cudaError_t launch_udt(const HqChain* chains, int n, int side, int b, int Nmax, 
   return cudaGetLastError();
 }
 cudaError_t launch_invert(const HqChain* chains, int n, int b, int which, int Nmax, bool resident, cudaStream_t st) {
-  const size_t bytes = smem_matrix_bytes(Nmax, resident, 2 * Nmax + 64);
+  const size_t bytes = smem_matrix_bytes(Nmax, resident, 3 * Nmax + 64);
   k_invert<<<n, HQ_THREADS, bytes, st>>>(chains, n, b, which, resident ? 1 : 0);
   return cudaGetLastError();
 }
@@ -1090,7 +1382,7 @@ cudaError_t launch_dyn_start(const HqChain* chains, int n, cudaStream_t st) {
 cudaError_t launch_dyn_slices(const HqChain* chains, int n, int b, int flags, int Nmax, bool resident, cudaStream_t st) {
   const size_t bytes = smem_matrix_bytes(Nmax, resident, 8 * (((Nmax + 15) & ~15) + 4) + 64);
   dim3 grid(n, 3);
-  k_dyn_slices<<<grid, HQ_THREADS, bytes, st>>>(chains, n, b, flags, resident ? 1 : 0);
+  k_dyn_slices<<<grid, HQ_INT_THREADS, bytes, st>>>(chains, n, b, flags, resident ? 1 : 0);
   return cudaGetLastError();
 }
 cudaError_t launch_dyn_measure(const HqChain* chains, int n, int b, int last_only, cudaStream_t st) {
@@ -1103,7 +1395,7 @@ cudaError_t launch_dyn_store(const HqChain* chains, int n, int b, cudaStream_t s
 }
 cudaError_t launch_adj_interval(const HqChain* chains, int n, int b, int Nmax, bool resident, cudaStream_t st) {
   const size_t bytes = smem_matrix_bytes(Nmax, resident, 8 * (((Nmax + 15) & ~15) + 4) + 64);
-  k_adj_interval<<<n, HQ_THREADS, bytes, st>>>(chains, n, b, resident ? 1 : 0);
+  k_adj_interval<<<n, HQ_INT_THREADS, bytes, st>>>(chains, n, b, resident ? 1 : 0);
   return cudaGetLastError();
 }
 cudaError_t launch_adj_last(const HqChain* chains, int n, int b, cudaStream_t st) {

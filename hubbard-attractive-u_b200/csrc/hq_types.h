@@ -9,7 +9,8 @@
 
 #define HQ_MAX_L 16           // largest linear lattice size of the separable expK path
 #define HQ_MAX_N 1024         // largest N = L*L handled by any path
-#define HQ_THREADS 512        // threads of the per-chain kernels (16 warps)
+#define HQ_THREADS 512        // threads of the per-chain factorisation kernels (16 warps)
+#define HQ_INT_THREADS 256    // threads of the interval kernel (8 warps)
 
 // expK application modes (the reference's is_fft switch, include/dqmc_params.hpp:44)
 enum HqExpkMode { HQK_EXPK_DENSE = 0, HQK_EXPK_SEPARABLE = 1 };
