@@ -1325,21 +1325,35 @@ size_t smem_matrix_bytes(int Nmax, bool resident, int extra_doubles) {
   return (mat + (size_t)extra_doubles) * sizeof(double);
 }
 
-static cudaError_t set_smem(const void* fn, size_t bytes) {
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+// The dynamic shared-memory limit of a kernel is a per-device property of the function
+// shared by every context of the process: it is only ever raised, so that preparing a
+// context of small chains never lowers the limit an existing context of larger chains
+// launches with.
+constexpr int kMaxTrackedDevices = 64;
+constexpr int kTrackedKernels = 6;
+static size_t g_smem_set[kMaxTrackedDevices][kTrackedKernels];
+
+static cudaError_t raise_smem(int slot, const void* fn, size_t bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < kMaxTrackedDevices && g_smem_set[dev][slot] >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess && dev >= 0 && dev < kMaxTrackedDevices) g_smem_set[dev][slot] = bytes;
+  return e;
 }
 
-// sets the dynamic shared-memory limits of every per-chain kernel once (outside any
-// stream capture) for the largest chain of a context
+// sets the dynamic shared-memory limits of every per-chain kernel (outside any stream
+// capture) so that chains of up to Nmax sites can be launched
 cudaError_t prepare_kernels(int Nmax, int kmax, bool resident) {
   const size_t mat_stage = smem_matrix_bytes(Nmax, resident, 8 * (((Nmax + 15) & ~15) + 4) + 64);
   cudaError_t e;
-  if ((e = set_smem((const void*)k_interval, smem_interval_bytes(Nmax, kmax, resident))) != cudaSuccess) return e;
-  if ((e = set_smem((const void*)k_bchain, mat_stage)) != cudaSuccess) return e;
-  if ((e = set_smem((const void*)k_udt, smem_matrix_bytes(Nmax, resident, 5 * Nmax + 64))) != cudaSuccess) return e;
-  if ((e = set_smem((const void*)k_invert, smem_matrix_bytes(Nmax, resident, 3 * Nmax + 64))) != cudaSuccess) return e;
-  if ((e = set_smem((const void*)k_dyn_slices, mat_stage)) != cudaSuccess) return e;
-  if ((e = set_smem((const void*)k_adj_interval, mat_stage)) != cudaSuccess) return e;
+  if ((e = raise_smem(0, (const void*)k_interval, smem_interval_bytes(Nmax, kmax, resident))) != cudaSuccess) return e;
+  if ((e = raise_smem(1, (const void*)k_bchain, mat_stage)) != cudaSuccess) return e;
+  if ((e = raise_smem(2, (const void*)k_udt, smem_matrix_bytes(Nmax, resident, 5 * Nmax + 64))) != cudaSuccess) return e;
+  if ((e = raise_smem(3, (const void*)k_invert, smem_matrix_bytes(Nmax, resident, 3 * Nmax + 64))) != cudaSuccess) return e;
+  if ((e = raise_smem(4, (const void*)k_dyn_slices, mat_stage)) != cudaSuccess) return e;
+  if ((e = raise_smem(5, (const void*)k_adj_interval, mat_stage)) != cudaSuccess) return e;
   return cudaSuccess;
 }
 
