@@ -26,6 +26,7 @@ EXPORTS = [
     "hq_get_wrap_errors", "hq_get_estimators", "hq_get_dynamic_estimators", "hq_reset_estimators",
     "hq_ratio_log", "hq_logdet_adjoint", "hq_capture_graph", "hq_launch_graph", "hq_get_config",
     "hq_upload_fields_i8", "hq_download_fields_i8", "hq_get_stream", "hq_profile_enable", "hq_profile_collect",
+    "hq_equaltime_g_noalloc",
 ]
 PROFILE_CLASSES = ["interval", "bchain", "udt", "gemm", "invert", "measure", "dynamic", "adjoint"]
 
@@ -92,6 +93,7 @@ def lib():
             "hq_get_stream": [vp, ctypes.POINTER(vp)],
             "hq_profile_enable": [vp, c_int],
             "hq_profile_collect": [vp, dp, ctypes.POINTER(c_ll), c_int],
+            "hq_equaltime_g_noalloc": [c_int, c_dbl, c_dbl, c_dbl, c_dbl, c_int, c_int, vp, vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

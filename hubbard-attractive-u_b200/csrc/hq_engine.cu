@@ -1132,3 +1132,193 @@ int hq_logdet_adjoint(hq_ctx* c, double* out, double* logdet) {
 }
 
 }  // extern "C"
+
+// =======================================================================================
+//  hq_equaltime_g_noalloc: an entry point that allocates no device memory.
+//
+//  Some callers cannot call cudaMalloc: code that runs inside a region being captured into
+//  a CUDA graph by someone else, runtimes that hand out a fixed pool of device memory up
+//  front and forbid further allocations, or embedded hosts that must never fail on an
+//  out-of-memory path after start-up. For them, hq_equaltime_g_noalloc computes the
+//  equal-time Green's function G(0,0) = (1 + B(nt-1)...B(0))^-1 of one chain from Ising
+//  fields already on the device, with every temporary (the UDV stack, the work matrices,
+//  the chain descriptor and the GEMM job lists) held in one file-scope device array of
+//  fixed size. The work is the kernel sequence of hq_init_stacks_and_g.
+// =======================================================================================
+namespace {
+
+// Scratch of the no-allocation entry point (hq_equaltime_g_noalloc). Every GPU that loads the library holds these
+// bytes until the process exits. Limits: N = nl*nl <= 64 and ceil(nt / pace) <= 16.
+constexpr size_t kScratchBytes = size_t(4) << 20;
+constexpr int kMaxN = 64;
+constexpr int kMaxStab = 16;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+void* g_scratch_addr[kMaxDevices] = {nullptr};  // device address of the scratch, per device
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;  // reported by hq_last_error()
+  return code;
+}
+
+// exp(dt t H_1d) of the L-site periodic chain is circulant:
+// a[d] = (1/L) sum_k exp(2 dt t cos(2 pi k / L)) cos(2 pi k d / L)
+void circulant(int L, double dt_t, double* a) { circulant_exp(L, dt_t, a); }
+size_t up256(size_t b) { return align256(b); }
+HqGemmJob job(int N, const double* A, int ta, const double* B, int tb, double* C) { return make_job(N, A, ta, B, tb, C); }
+
+}  // namespace
+
+extern "C" HQ_API int hq_equaltime_g_noalloc(int nl, double nnt, double u, double mu, double beta, int nt, int pace,
+                                             const signed char* fields_dev, double* g_dev, void* stream) {
+  // ---- argument and size checks (include/dqmc_parser.hpp:124-132 plus the scratch limits) ----
+  if (!fields_dev || !g_dev) return set_error(HQ_E_INVALID, "hq_equaltime_g_noalloc: null device pointer");
+  if (nl < 1 || nt < 1 || pace < 1 || u < 0 || beta < 0)
+    return set_error(HQ_E_INVALID, "hq_equaltime_g_noalloc: parameter out of range");
+  const int N = nl * nl;
+  const int n_stab = (nt % pace == 0) ? nt / pace : nt / pace + 1;
+  if (N > kMaxN)
+    return set_error(HQ_E_RANGE, "hq_equaltime_g_noalloc: nl*nl = " + std::to_string(N) +
+                                     " exceeds the scratch limit of 64 sites");
+  if (n_stab > kMaxStab)
+    return set_error(HQ_E_RANGE, "hq_equaltime_g_noalloc: ceil(nt/pace) = " + std::to_string(n_stab) +
+                                     " exceeds the scratch limit of 16 stack entries");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+    return set_error(HQ_E_CUDA, "hq_equaltime_g_noalloc: no current CUDA device");
+  // ---- set-up, once per device, with that device current: the scratch's device address ----
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return set_error(HQ_E_CUDA, std::string("hq_equaltime_g_noalloc: cudaGetSymbolAddress: ") +
+                                      cudaGetErrorString(e));
+    g_scratch_addr[dev] = p;
+  }
+  char* base = static_cast<char*>(g_scratch_addr[dev]);
+
+  // ---- scratch layout ----
+  const size_t NN = size_t(N) * N, mat = NN * sizeof(double);
+  size_t off = 0;
+  auto take = [&](size_t bytes) { const size_t o = off; off += up256(bytes); return o; };
+  const size_t o_desc = take(sizeof(HqChain));
+  const int njobs = n_stab + 4;
+  const size_t o_jobs = take(sizeof(HqGemmJob) * njobs);
+  const size_t o_U = take(2 * size_t(n_stab) * mat);
+  const size_t o_D = take(2 * size_t(n_stab) * N * sizeof(double));
+  const size_t o_Vt = take(2 * size_t(n_stab) * mat);
+  const size_t o_X = take(mat);
+  size_t o_W[4];
+  for (auto& w : o_W) w = take(mat);
+  const size_t o_I = take(mat);
+  const size_t o_one = take(N * sizeof(double));
+  const size_t o_E = take(2 * mat);
+  const size_t o_acc = take(HQ_ACC_COUNT * sizeof(double));
+  const size_t o_rng = take(sizeof(uint32_t));
+  if (off > kScratchBytes) return set_error(HQ_E_RANGE, "hq_equaltime_g_noalloc: scratch layout exceeds 4 MiB");
+  auto ptr = [&](size_t o) { return reinterpret_cast<double*>(base + o); };
+
+  // ---- model constants (src/hubbard.cpp:25-49) ----
+  const double dt = beta / nt;
+  const double alpha = std::acosh(std::exp(0.5 * dt * u));
+  HqChain d;
+  std::memset(&d, 0, sizeof(d));
+  d.N = N; d.L = nl; d.nt = nt; d.pace = pace; d.n_stab = n_stab;
+  d.expk_mode = (nl <= HQ_MAX_L) ? HQK_EXPK_SEPARABLE : HQK_EXPK_DENSE;
+  d.kmax = 4; d.active = 1;
+  d.alpha = alpha; d.dt = dt;
+  d.delta_p = std::exp(-2 * alpha) - 1;
+  d.delta_m = std::exp(2 * alpha) - 1;
+  d.ev_p = std::exp(alpha);
+  d.ev_m = std::exp(-alpha);
+  d.sep_c = std::exp(dt * mu);
+  d.sep_ci = std::exp(-dt * mu);
+  circulant(nl, dt * nnt, d.sep_a);
+  circulant(nl, -dt * nnt, d.sep_ai);
+  d.expK = ptr(o_E);
+  d.inv_expK = ptr(o_E) + NN;
+  d.G = g_dev;
+  d.fields = reinterpret_cast<int8_t*>(const_cast<signed char*>(fields_dev));
+  d.rng = reinterpret_cast<uint32_t*>(base + o_rng);
+  d.X = ptr(o_X);
+  d.stackU = ptr(o_U);
+  d.stackD = ptr(o_D);
+  d.stackVt = ptr(o_Vt);
+  d.W0 = ptr(o_W[0]); d.W1 = ptr(o_W[1]); d.W2 = ptr(o_W[2]); d.W3 = ptr(o_W[3]);
+  d.W4 = d.W3; d.W5 = d.W3;  // not used by this sequence
+  d.acc = ptr(o_acc);
+
+  // host images of the constant inputs: dense expK, identity, ones (copied on the caller's
+  // stream; pageable sources are consumed before cudaMemcpyAsync returns)
+  std::vector<double> a(nl), ai(nl), E(2 * NN), I(NN, 0.0), one(N, 1.0);
+  circulant(nl, dt * nnt, a.data());
+  circulant(nl, -dt * nnt, ai.data());
+  for (int j = 0; j < N; ++j)
+    for (int i = 0; i < N; ++i) {
+      const int dx = ((i % nl) - (j % nl) + nl) % nl, dy = ((i / nl) - (j / nl) + nl) % nl;
+      E[i + size_t(j) * N] = d.sep_c * a[dx] * a[dy];
+      E[NN + i + size_t(j) * N] = d.sep_ci * ai[dx] * ai[dy];
+    }
+  for (int k = 0; k < N; ++k) I[k + size_t(k) * N] = 1.0;
+
+  // ---- batched GEMM jobs: stack pushes, then the builder with an empty left stack ----
+  std::vector<HqGemmJob> jobs;
+  const double* Iid = ptr(o_I);
+  const double* ones = ptr(o_one);
+  for (int b = 0; b < n_stab; ++b) {
+    const double* prev = (b == 0) ? Iid : d.stackVt + (size_t(n_stab) + (b - 1)) * NN;
+    jobs.push_back(job(N, d.W0, 0, prev, 0, d.stackVt + (size_t(n_stab) + b) * NN));
+  }
+  const double* UR = d.stackU + (size_t(n_stab) + n_stab - 1) * NN;
+  const double* DR = d.stackD + (size_t(n_stab) + n_stab - 1) * N;
+  const double* VtR = d.stackVt + (size_t(n_stab) + n_stab - 1) * NN;
+  HqGemmJob b1 = job(N, Iid, 1, UR, 0, d.W1);
+  b1.rs = ones; b1.rs_mode = 2; b1.cs = DR; b1.cs_mode = 2;
+  HqGemmJob b2 = job(N, Iid, 0, VtR, 1, d.W1);
+  b2.rs = ones; b2.rs_mode = 3; b2.cs = DR; b2.cs_mode = 3; b2.beta = 1.0;
+  HqGemmJob b3 = job(N, d.W1, 0, Iid, 1, d.W2);
+  b3.ks = ones; b3.ks_mode = 2;
+  HqGemmJob b4 = job(N, UR, 0, d.W2, 0, g_dev);
+  b4.ks = DR; b4.ks_mode = 2;
+  jobs.push_back(b1);
+  jobs.push_back(b2);
+  jobs.push_back(b3);
+  jobs.push_back(b4);
+
+  // ---- upload (no allocation) and launch ----
+  cudaError_t e = cudaSuccess;
+  HqChain* d_desc = reinterpret_cast<HqChain*>(base + o_desc);
+  HqGemmJob* d_jobs = reinterpret_cast<HqGemmJob*>(base + o_jobs);
+  if ((e = cudaMemcpyAsync(d_desc, &d, sizeof(d), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(HqGemmJob), cudaMemcpyHostToDevice, st)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(ptr(o_E), E.data(), E.size() * sizeof(double), cudaMemcpyHostToDevice, st)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(ptr(o_I), I.data(), I.size() * sizeof(double), cudaMemcpyHostToDevice, st)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(ptr(o_one), one.data(), one.size() * sizeof(double), cudaMemcpyHostToDevice, st)) !=
+          cudaSuccess ||
+      (e = cudaMemsetAsync(ptr(o_acc), 0, HQ_ACC_COUNT * sizeof(double), st)) != cudaSuccess)
+    return set_error(HQ_E_CUDA, std::string("hq_equaltime_g_noalloc: upload: ") + cudaGetErrorString(e));
+  // the kernels' shared-memory limits (raised only, and only when an earlier context of
+  // smaller chains left them below this size; no allocation)
+  if ((e = hq::prepare_kernels(N, 4, true)) != cudaSuccess)
+    return set_error(HQ_E_CUDA, std::string("hq_equaltime_g_noalloc: kernel limits: ") + cudaGetErrorString(e));
+  for (int b = 0; b < n_stab && e == cudaSuccess; ++b) {
+    // src/dqmc_core.cpp:67-87: B^T products from t = nt down to 1, pushed every pace slices
+    e = hq::launch_bchain(d_desc, 1, HQ_DOWN, b, N, true, st);
+    if (e == cudaSuccess) e = hq::launch_udt(d_desc, 1, 1, b, N, true, st);
+    if (e == cudaSuccess) e = hq::launch_gemm(d_jobs + b, 1, N, N, st);
+  }
+  // src/dqmc_core.cpp:89-97 with stable_numerics.hpp:186-239: G = (1 + right^T)^-1
+  const int jb = n_stab;
+  if (e == cudaSuccess) e = hq::launch_gemm(d_jobs + jb, 1, N, N, st);
+  if (e == cudaSuccess) e = hq::launch_gemm(d_jobs + jb + 1, 1, N, N, st);
+  if (e == cudaSuccess) e = hq::launch_invert(d_desc, 1, n_stab - 1, 0, N, true, st);
+  if (e == cudaSuccess) e = hq::launch_gemm(d_jobs + jb + 2, 1, N, N, st);
+  if (e == cudaSuccess) e = hq::launch_gemm(d_jobs + jb + 3, 1, N, N, st);
+  if (e != cudaSuccess) return set_error(HQ_E_CUDA, std::string("hq_equaltime_g_noalloc: launch: ") + cudaGetErrorString(e));
+  return HQ_OK;
+}

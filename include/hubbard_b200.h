@@ -172,6 +172,22 @@ HQ_API int hq_get_config(hq_ctx* ctx, int chain, int* expk_mode, int* delay_dept
 HQ_API int hq_upload_fields_i8(hq_ctx* ctx, const signed char* fields_all);
 HQ_API int hq_download_fields_i8(hq_ctx* ctx, signed char* fields_all);
 
+/* Equal-time G(0,0) = (1 + B(nt-1)...B(0))^-1 of one chain, computed without allocating any
+ * device memory, for callers that cannot call cudaMalloc (inside someone else's stream
+ * capture, under a fixed device-memory budget handed out up front, or on hosts that must
+ * not meet an out-of-memory path after start-up). No counterpart in the reference.
+ *   fields_dev: device array of nt*N int8 fields (+1/-1, [nt][N]); g_dev: device output,
+ *   N*N doubles, column-major; stream: cudaStream_t (NULL = default stream).
+ * Limits: N = nl*nl <= 64 and ceil(nt / stabilization_pace) <= 16; larger sizes return
+ * HQ_E_RANGE with a message in hq_last_error(). All temporaries live in one 4 MiB device
+ * array defined in the library, which every GPU that loads the library keeps until exit;
+ * its first call on a device looks up that array's device address and raises the
+ * kernels' shared-memory limits where needed (call it once before any stream capture). Calls share the array: calls that overlap on the GPU race, so
+ * serialise them (one stream, or stream ordering). The work is enqueued on `stream`. */
+HQ_API int hq_equaltime_g_noalloc(int nl, double nnt, double u, double mu, double beta, int nt,
+                                  int stabilization_pace, const signed char* fields_dev, double* g_dev,
+                                  void* stream);
+
 #ifdef __cplusplus
 }
 #endif
