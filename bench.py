@@ -40,6 +40,7 @@ SEED0 = 1000
 
 
 def chain_params(rank, n=N_CHAINS, expk_mode=-1):
+    """The metric's chains: seeds 1000 + c, c counted across ranks."""
     return [dict(CFG, seed=SEED0 + rank * n + c, expk_mode=expk_mode) for c in range(n)]
 
 
@@ -205,8 +206,8 @@ def run_gpu(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    n = N_CHAINS
-    peak = fp64_peak_tflops(torch, local)
+    n = args.chains
+    peak = fp64_peak_tflops(torch, local) if not args.no_peak else None
 
     eng = hq.Engine(chain_params(rank, n), device=local)
     eng.fields_random()
@@ -271,7 +272,7 @@ def run_gpu(args):
         flops_per_launch = None
     achieved = (flops_per_launch / (avg_launch_ms * 1e-3) / 1e12) if flops_per_launch else None
     roofline = {"bound": "tensor", "kernel": f"k_{dom_name}", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "unit": "TFLOP/s", "frac": (achieved / peak) if (achieved and peak) else None, "traffic": None,
                 "peak_source": "measured cuBLAS DGEMM 8192^3 FP64 on this GPU (FP64 has no entry in MEASURED_PEAKS.json)",
                 "launch_ms_avg": avg_launch_ms, "launches": int(cnt_cls[dom]),
                 "device_ms_by_class": {nm: round(float(v), 3) for nm, v in zip(hq.capi.PROFILE_CLASSES, ms_cls)},
@@ -281,11 +282,12 @@ def run_gpu(args):
 
     # ---- end to end through the C ABI from pinned host buffers ----
     nbytes = n * CFG["nt"] * CFG["nl"] ** 2
+    e2e_value = None
     host_fields = torch.empty(nbytes, dtype=torch.int8, pin_memory=True)
     eng.download_fields_i8(host_fields.data_ptr())
     eng.sync()
     host_est = np.zeros((n, 6))
-    e2e_steps = max(2, min(args.steps, 6))
+    e2e_steps = 0 if args.no_e2e else max(2, min(args.steps, 6))
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -303,11 +305,12 @@ def run_gpu(args):
         t = torch.tensor([e2e_s], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = world * n * e2e_steps / e2e_s
+    if e2e_steps:
+        e2e_value = world * n * e2e_steps / e2e_s
 
     # ---- the plain single-chain GPU path (the 20x bar's denominator) ----
     single = None
-    if rank == 0:
+    if rank == 0 and not args.no_single:
         one = hq.Engine(chain_params(rank, 1), device=local)
         one.fields_random()
         one.init()
@@ -352,9 +355,10 @@ def run_gpu(args):
                        "l2": "working set per GPU ~1.8 GB of chain state (> 126 MB L2)"},
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "sweeps/s", "h2d_bytes_per_step": nbytes,
-                    "d2h_bytes_per_step": nbytes + n * 6 * 8,
-                    "step": "h2d fields -> hq_init_stacks_and_g -> hq_sweep(up) -> d2h fields + estimators"},
+            "e2e": ({"value": e2e_value, "unit": "sweeps/s", "h2d_bytes_per_step": nbytes,
+                     "d2h_bytes_per_step": nbytes + n * 6 * 8,
+                     "step": "h2d fields -> hq_init_stacks_and_g -> hq_sweep(up) -> d2h fields + estimators"}
+                    if e2e_value else None),
             "gpu_launches": gpu_launches,
             "clocks": clk,
             "single_chain_gpu": {"value": single, "unit": "sweeps/s",
@@ -377,6 +381,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of the CPU baseline sample")
+    ap.add_argument("--chains", type=int, default=N_CHAINS, help="chains per GPU (256 is the metric's)")
+    ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak probe")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--no-single", action="store_true", help="skip the single-chain leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -193,7 +193,7 @@ namespace {
 enum Phase {
   PH_PUSH = 0,   // Vt_new = T * Vt_prev
   PH_B1, PH_B2, PH_B3, PH_B4,                       // equal-time builder
-  PH_D3, PH_D4, PH_D5, PH_D6, PH_D7, PH_D8, PH_D9, PH_D10, PH_D11, PH_D12,  // displaced builder
+  PH_D3, PH_D4, PH_D5, PH_D6,  // displaced builder
   PH_LOGDET,
 };
 
@@ -286,35 +286,24 @@ void build_jobs(hq_ctx* c) {
           push_job(PH_B4, k);
         }
         if (dir == 3) {
-          // G(t,t) fresh -> W3 ; G(t,0) fresh -> W0 ; G(0,t) fresh -> W4
+          // G(t,t) fresh -> W3, G(t,0) fresh -> W0, G(0,t) fresh -> W4, with
+          // Y = W1^-1 dlmax^-1 U_L^T (W2, from PH_B3) and W1 = T1^-1:
+          //   G(t,t) =  U_R drmax^-1 Y
+          //   G(t,0) =  U_R drmax^-1 T1^-1 dlmin Vt_L            (stable_numerics.hpp:300-301)
+          //   G(0,t) = -B(beta,t) G(t,t) = -Vt_R^T drmin Y         (C = Vt_R^T D_R U_R^T and
+          //            D_R drmax^-1 = drmin: no inverse of the V factors is needed)
           HqGemmJob k = make_job(N, Rv.U, 0, d.W2, 0, d.W3);
           k.ks = Rv.D; k.ks_mode = 2;
           push_job(PH_D3, k);
-          HqGemmJob j5 = make_job(N, d.W1, 0, Lv.Vt, 0, d.W2);  // W1^-1 dlmin Vt_L
+          HqGemmJob j5 = make_job(N, d.W1, 0, Lv.Vt, 0, d.W5);  // T1^-1 dlmin Vt_L
           j5.ks = Lv.D; j5.ks_mode = 3;
           push_job(PH_D4, j5);
-          HqGemmJob j6 = make_job(N, Rv.U, 0, d.W2, 0, d.W0);  // U_R drmax^-1 (...)
+          HqGemmJob j6 = make_job(N, Rv.U, 0, d.W5, 0, d.W0);  // U_R drmax^-1 (...)
           j6.ks = Rv.D; j6.ks_mode = 2;
           push_job(PH_D5, j6);
-          // M = Vt_L Vt_R^T -> W1 (then inverted)
-          push_job(PH_D6, make_job(N, Lv.Vt, 0, Rv.Vt, 1, d.W1));
-          // T3 = drmin (U_R^T U_L) dlmin + drmax^-1 M^-1 dlmax^-1 -> W2 (two jobs)
-          HqGemmJob j8 = make_job(N, Rv.U, 1, Lv.U, 0, d.W2);
-          j8.rs = Rv.D; j8.rs_mode = 3; j8.cs = Lv.D; j8.cs_mode = 3;
-          push_job(PH_D7, j8);
-          HqGemmJob j9 = make_job(N, c->ident[N].first, 0, d.W1, 0, d.W2);
-          j9.rs = Rv.D; j9.rs_mode = 2; j9.cs = Lv.D; j9.cs_mode = 2; j9.beta = 1.0;
-          push_job(PH_D8, j9);
-          // W5 = Vt_L (copy, then inverted)
-          push_job(PH_D9, make_job(N, c->ident[N].first, 0, Lv.Vt, 0, d.W5));
-          // W1 = T3^-1 drmin U_R^T
-          HqGemmJob j11 = make_job(N, d.W2, 0, Rv.U, 1, d.W1);
-          j11.ks = Rv.D; j11.ks_mode = 3;
-          push_job(PH_D10, j11);
-          // G(0,t) = -Vt_L^-1 dlmax^-1 W1 -> W4
-          HqGemmJob j12 = make_job(N, d.W5, 0, d.W1, 0, d.W4);
-          j12.ks = Lv.D; j12.ks_mode = 2; j12.alpha = -1.0;
-          push_job(PH_D11, j12);
+          HqGemmJob j7 = make_job(N, Rv.Vt, 1, d.W2, 0, d.W4);  // -Vt_R^T drmin Y
+          j7.ks = Rv.D; j7.ks_mode = 3; j7.alpha = -1.0;
+          push_job(PH_D6, j7);
         }
       }
       for (auto& kv : ph) add_phase(kv.first, dir, b, kv.second);
@@ -422,19 +411,11 @@ void issue_sweep(hq_ctx* c, int dir, int flags) {
       run_jobs(c, PH_B1, 3, b);
       run_jobs(c, PH_B2, 3, b);
       { ProfScope ps(c, PC_INVERT); HQ_CUDA(hq::launch_invert(c->d_desc, c->n, b, 0, c->Nmax, c->resident, c->stream)); }
-      run_jobs(c, PH_B3, 3, b);   // W2 = W1^-1 dlmax^-1 U_L^T
+      run_jobs(c, PH_B3, 3, b);   // W2 = Y = T1^-1 dlmax^-1 U_L^T
       run_jobs(c, PH_D3, 3, b);   // W3 = G(t,t)
-      run_jobs(c, PH_D4, 3, b);   // W2 = W1^-1 dlmin Vt_L
+      run_jobs(c, PH_D4, 3, b);   // W5 = T1^-1 dlmin Vt_L
       run_jobs(c, PH_D5, 3, b);   // W0 = G(t,0)
-      run_jobs(c, PH_D6, 3, b);   // W1 = Vt_L Vt_R^T
-      { ProfScope ps(c, PC_INVERT); HQ_CUDA(hq::launch_invert(c->d_desc, c->n, b, 0, c->Nmax, c->resident, c->stream)); }
-      run_jobs(c, PH_D7, 3, b);   // W2 = drmin U_R^T U_L dlmin
-      run_jobs(c, PH_D8, 3, b);   // W2 += drmax^-1 W1 dlmax^-1
-      { ProfScope ps(c, PC_INVERT); HQ_CUDA(hq::launch_invert(c->d_desc, c->n, b, 1, c->Nmax, c->resident, c->stream)); }
-      run_jobs(c, PH_D9, 3, b);   // W5 = Vt_L
-      { ProfScope ps(c, PC_INVERT); HQ_CUDA(hq::launch_invert(c->d_desc, c->n, b, 3, c->Nmax, c->resident, c->stream)); }
-      run_jobs(c, PH_D10, 3, b);  // W1 = W2 drmin U_R^T
-      run_jobs(c, PH_D11, 3, b);  // W4 = -W5 dlmax^-1 W1 = G(0,t)
+      run_jobs(c, PH_D6, 3, b);   // W4 = G(0,t)
       { ProfScope ps(c, PC_DYN); HQ_CUDA(hq::launch_dyn_commit(c->d_desc, c->n, b, c->stream)); }
       { ProfScope ps(c, PC_DYN); HQ_CUDA(hq::launch_dyn_store(c->d_desc, c->n, b, c->stream)); }
       { ProfScope ps(c, PC_DYN); HQ_CUDA(hq::launch_dyn_measure(c->d_desc, c->n, b, 0, c->stream)); }
@@ -512,7 +493,8 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   HQ_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
   const size_t budget = size_t(smem_optin) - 4096;  // static shared memory of the kernels
   c->resident = hq::smem_interval_bytes(c->Nmax, 4, true) <= budget &&
-                hq::smem_matrix_bytes(c->Nmax, true, 8 * (((c->Nmax + 15) & ~15) + 4) + 64) <= budget;
+                hq::smem_matrix_bytes(c->Nmax, true, 8 * (((c->Nmax + 15) & ~15) + 4) + 64) <= budget &&
+                hq::smem_invert_bytes(c->Nmax, true) <= budget && hq::smem_udt_bytes(c->Nmax, true) <= budget;
   int kfit = 4;
   for (int k : {16, 8, 4})
     if (hq::smem_interval_bytes(c->Nmax, k, c->resident) <= budget) { kfit = k; break; }

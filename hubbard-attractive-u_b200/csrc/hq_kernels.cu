@@ -83,11 +83,13 @@ __device__ void copy_mat(double* dst, int ldd, const double* src, int lds, int N
 //  accepted updates are kept as G = G0 + X Y (X: N x k, Y: k x N) and flushed into G0
 //  with DMMA when k reaches kmax and at the end of the slice.
 // ---------------------------------------------------------------------------------
-__device__ void flush_panels(double* G, int ld, int N, const double* X, int ldx, const double* Y, int ldy, int k) {
-  // G += X Y by 16 x 32 strips (four 16 x 8 DMMA tiles sharing the A fragments)
+// G[0:M, 0:Nc] += X[0:M, 0:k] Y[0:k, 0:Nc]  (X column-major ldx, Y row-major ldy), by 16 x 32
+// strips of four 16 x 8 DMMA tiles that share the A fragments
+__device__ void rank_update(double* G, int ld, int M, int Nc, const double* X, int ldx, const double* Y, int ldy,
+                            int k) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int g = lane >> 2, q = lane & 3;
-  const int mt = (N + 15) / 16, ns = (N + 31) / 32;
+  const int mt = (M + 15) / 16, ns = (Nc + 31) / 32;
   const int strips = mt * ns;
   for (int st = warp; st < strips; st += nwarps) {
     const int r0 = (st % mt) * 16, c0 = (st / mt) * 32;
@@ -96,32 +98,37 @@ __device__ void flush_panels(double* G, int ld, int N, const double* X, int ldx,
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       const int c = c0 + t * 8 + 2 * q;
-      acc[t][0] = (r < N && c < N) ? G[r + (size_t)c * ld] : 0.0;
-      acc[t][1] = (r < N && c + 1 < N) ? G[r + (size_t)(c + 1) * ld] : 0.0;
-      acc[t][2] = (r + 8 < N && c < N) ? G[r + 8 + (size_t)c * ld] : 0.0;
-      acc[t][3] = (r + 8 < N && c + 1 < N) ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
+      acc[t][0] = (r < M && c < Nc) ? G[r + (size_t)c * ld] : 0.0;
+      acc[t][1] = (r < M && c + 1 < Nc) ? G[r + (size_t)(c + 1) * ld] : 0.0;
+      acc[t][2] = (r + 8 < M && c < Nc) ? G[r + 8 + (size_t)c * ld] : 0.0;
+      acc[t][3] = (r + 8 < M && c + 1 < Nc) ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
     }
     for (int m0 = 0; m0 < k; m0 += 4) {
       const int m = m0 + q;
       const bool mk = m < k;
-      const double a0 = (r < N && mk) ? X[r + m * ldx] : 0.0;
-      const double a1 = (r + 8 < N && mk) ? X[r + 8 + m * ldx] : 0.0;
+      const double a0 = (r < M && mk) ? X[r + m * ldx] : 0.0;
+      const double a1 = (r + 8 < M && mk) ? X[r + 8 + m * ldx] : 0.0;
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int cb = c0 + t * 8 + g;
-        const double b0 = (cb < N && mk) ? Y[m * ldy + cb] : 0.0;
+        const double b0 = (cb < Nc && mk) ? Y[m * ldy + cb] : 0.0;
         dmma_16x8x4(acc[t], a0, a1, b0);
       }
     }
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       const int c = c0 + t * 8 + 2 * q;
-      if (r < N && c < N) G[r + (size_t)c * ld] = acc[t][0];
-      if (r < N && c + 1 < N) G[r + (size_t)(c + 1) * ld] = acc[t][1];
-      if (r + 8 < N && c < N) G[r + 8 + (size_t)c * ld] = acc[t][2];
-      if (r + 8 < N && c + 1 < N) G[r + 8 + (size_t)(c + 1) * ld] = acc[t][3];
+      if (r < M && c < Nc) G[r + (size_t)c * ld] = acc[t][0];
+      if (r < M && c + 1 < Nc) G[r + (size_t)(c + 1) * ld] = acc[t][1];
+      if (r + 8 < M && c < Nc) G[r + 8 + (size_t)c * ld] = acc[t][2];
+      if (r + 8 < M && c + 1 < Nc) G[r + 8 + (size_t)(c + 1) * ld] = acc[t][3];
     }
   }
+}
+
+// G += X Y on the full N x N matrix (the flush of the delayed Metropolis panels)
+__device__ void flush_panels(double* G, int ld, int N, const double* X, int ldx, const double* Y, int ldy, int k) {
+  rank_update(G, ld, N, N, X, ldx, Y, ldy, k);
 }
 
 // barrier of the decision team (warps 0-3 of the interval kernel)
@@ -637,69 +644,135 @@ k_bchain(const HqChain* __restrict__ chains, int nchains, int dir, int b, int re
 }
 
 // ---------------------------------------------------------------------------------
-//  k_udt: X P = Q R (column-pivoted Householder QR in LAPACK dgeqp3/dlaqp2 order), then
-//  D = |diag R|, T = D^-1 R P^T, and Q formed in place (dorg2r order).
+//  k_udt: UDV factorisation X P = Q R of the stack push, X = Q D T with D = |diag R| and
+//  T = D^-1 R P^T (the role of dgesvd in include/utils/svd_stack.hpp:107-175).
+//  P sorts the columns of X by decreasing norm once ("pre-pivoting", C. Bauer, Fast and
+//  stable determinant quantum Monte Carlo, SciPost Phys. Core 2, 011 (2020)); the QR of
+//  the sorted matrix is blocked Householder in panels of kQB columns with compact-WY
+//  trailing updates A <- (I - V T^T V^T) A, whose two products run on DMMA; Q is formed
+//  in place by the same blocks backwards (Q = B_0 B_1 ..., B_p = I - V_p T_p V_p^T).
 //  Output: U (= Q) and D into stack entry b of the pushing stack, T into W0.
-//  Warp 0 does the serial part of every step (pivot, column swap, reflector); all warps
-//  then update the trailing columns, four columns per warp at a time, and downdate the
-//  partial column norms.
 // ---------------------------------------------------------------------------------
-__device__ inline void householder_trailing(double* A, int ld, int N, int i, double ti, double* vn1, double* vn2,
-                                            bool downdate, bool v_implicit_one) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const double tol3z = 1.4901161193847656e-08;  // sqrt(eps)
-  for (int j0 = i + 1 + warp * 4; j0 < N; j0 += nwarps * 4) {
-    double w[4] = {0.0, 0.0, 0.0, 0.0};
-    if (ti != 0.0) {
-      for (int r = i + lane; r < N; r += 32) {
-        const double v = (r == i && v_implicit_one) ? 1.0 : A[r + (size_t)i * ld];
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if (j0 + q < N) w[q] = fma(v, A[r + (size_t)(j0 + q) * ld], w[q]);
+constexpr int kQB = 16;
+
+// unblocked Householder QR of the panel columns [p0, p1) (rows p0..N-1), dlarfg convention
+__device__ void qr_panel(double* A, int ld, int N, int p0, int p1, double* tau) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c = p0; c < p1; ++c) {
+    if (warp == 0) {
+      double xs = 0.0;
+      for (int r = c + 1 + lane; r < N; r += 32) { const double v = A[r + (size_t)c * ld]; xs = fma(v, v, xs); }
+      xs = warp_sum(xs);
+      const double alpha = A[c + (size_t)c * ld];
+      double ti = 0.0, beta = alpha;
+      if (xs > 0.0) {
+        beta = -copysign(hypot(alpha, sqrt(xs)), alpha);
+        ti = (beta - alpha) / beta;
+        const double sc = 1.0 / (alpha - beta);
+        for (int r = c + 1 + lane; r < N; r += 32) A[r + (size_t)c * ld] *= sc;
       }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) w[q] = warp_sum(w[q]) * ti;
-      for (int r = i + lane; r < N; r += 32) {
-        const double v = (r == i && v_implicit_one) ? 1.0 : A[r + (size_t)i * ld];
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if (j0 + q < N) A[r + (size_t)(j0 + q) * ld] = fma(-w[q], v, A[r + (size_t)(j0 + q) * ld]);
-      }
+      __syncwarp();
+      if (lane == 0) { A[c + (size_t)c * ld] = beta; tau[c] = ti; }
     }
-    if (!downdate) continue;
-    __syncwarp();
-    // partial norm downdate of the (up to) four columns, lane q for column j0 + q
-    bool need = false;
-    {
-      const int j = j0 + lane;
-      if (lane < 4 && j < N) {
-        const double nv1 = vn1[j];
-        if (nv1 != 0.0) {
-          double temp = fabs(A[i + (size_t)j * ld]) / nv1;
-          temp = fmax(1.0 - temp * temp, 0.0);
-          const double r2 = nv1 / vn2[j];
-          if (temp * r2 * r2 <= tol3z) need = true;
-          else vn1[j] = nv1 * sqrt(temp);
+    __syncthreads();
+    // apply H_c to the remaining panel columns, one warp per column
+    const double ti = tau[c];
+    const int j = c + 1 + warp;
+    if (ti != 0.0 && j < p1) {
+      double w = (lane == 0) ? A[c + (size_t)j * ld] : 0.0;
+      for (int r = c + 1 + lane; r < N; r += 32) w = fma(A[r + (size_t)c * ld], A[r + (size_t)j * ld], w);
+      w = warp_sum(w) * ti;
+      if (lane == 0) A[c + (size_t)j * ld] -= w;
+      for (int r = c + 1 + lane; r < N; r += 32) A[r + (size_t)j * ld] = fma(-w, A[r + (size_t)c * ld], A[r + (size_t)j * ld]);
+    }
+    __syncthreads();
+  }
+}
+
+// V of the panel [p0, p0+m) with explicit unit diagonal and zeros above (columns >= m
+// zero), and the triangular factor T of H_p0 ... H_p0+m-1 = I - V T V^T
+__device__ void wy_factor(const double* A, int ld, int N, int p0, int m, const double* tau, double* Vb, int ldv,
+                          double* T, double* S) {
+  for (int q = threadIdx.x >> 5; q < kQB; q += blockDim.x >> 5)
+    for (int r = p0 + (threadIdx.x & 31); r < N; r += 32) {
+      const int c = p0 + q;
+      Vb[r + q * ldv] = (q >= m || r < c) ? 0.0 : (r == c ? 1.0 : A[r + (size_t)c * ld]);
+    }
+  __syncthreads();
+  // S = V^T V (upper triangle), rows >= p0 + b are the only nonzero overlap
+  for (int t = threadIdx.x; t < kQB * kQB; t += blockDim.x) {
+    const int a = t / kQB, bb = t % kQB;
+    double acc = 0.0;
+    if (a <= bb && bb < m)
+      for (int r = p0 + bb; r < N; ++r) acc = fma(Vb[r + a * ldv], Vb[r + bb * ldv], acc);
+    S[t] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int i = threadIdx.x;
+    for (int j = 0; j < kQB; ++j) {
+      if (i < kQB) {
+        double v = 0.0;
+        if (j < m) {
+          if (i == j) v = tau[p0 + j];
+          else if (i < j) {
+            double acc = 0.0;
+            for (int l = i; l < j; ++l) acc = fma(T[i * kQB + l], S[l * kQB + j], acc);
+            v = -tau[p0 + j] * acc;
+          }
         }
+        T[i * kQB + j] = v;
       }
-    }
-    unsigned nb = __ballot_sync(0xffffffffu, need);
-    while (nb) {
-      const int j = j0 + __ffs(nb) - 1;
-      nb &= nb - 1;
-      double s2 = 0.0;
-      for (int r = i + 1 + lane; r < N; r += 32) { const double v = A[r + (size_t)j * ld]; s2 = fma(v, v, s2); }
-      s2 = warp_sum(s2);
-      if (lane == 0) { vn1[j] = sqrt(s2); vn2[j] = vn1[j]; }
     }
   }
+  __syncthreads();
+}
+
+// A[p0:, col0:col0+nc] <- (I - V op(T) V^T) A[p0:, col0:col0+nc]; op(T) = T^T if trans
+__device__ void wy_apply(double* A, int ld, int N, int p0, const double* Vb, int ldv, const double* T, bool trans,
+                         double* W, int ldw, int col0, int nc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  // W = V^T A_sub (kQB x nc) with DMMA: m16 = the panel columns, k = rows p0..N-1
+  const int nt8 = (nc + 7) / 8;
+  for (int t = warp; t < nt8; t += nwarps) {
+    const int cb = t * 8 + g;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int r0 = p0; r0 < N; r0 += 4) {
+      const int r = r0 + q;
+      const double a0 = (r < N) ? Vb[r + g * ldv] : 0.0;
+      const double a1 = (r < N) ? Vb[r + (g + 8) * ldv] : 0.0;
+      const double b0 = (r < N && cb < nc) ? A[r + (size_t)(col0 + cb) * ld] : 0.0;
+      dmma_16x8x4(acc, a0, a1, b0);
+    }
+    const int c = t * 8 + 2 * q;
+    if (c < nc) { W[g * ldw + c] = acc[0]; W[(g + 8) * ldw + c] = acc[2]; }
+    if (c + 1 < nc) { W[g * ldw + c + 1] = acc[1]; W[(g + 8) * ldw + c + 1] = acc[3]; }
+  }
+  __syncthreads();
+  // W <- -op(T) W, one thread per column
+  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+    double w[kQB];
+#pragma unroll
+    for (int l = 0; l < kQB; ++l) w[l] = W[l * ldw + c];
+#pragma unroll
+    for (int i = 0; i < kQB; ++i) {
+      double acc = 0.0;
+#pragma unroll
+      for (int l = 0; l < kQB; ++l) acc = fma(trans ? T[l * kQB + i] : T[i * kQB + l], w[l], acc);
+      W[i * ldw + c] = -acc;
+    }
+  }
+  __syncthreads();
+  // A_sub += V (-op(T) W)
+  rank_update(A + p0 + (size_t)col0 * ld, ld, N - p0, nc, Vb + p0, ldv, W, ldw, kQB);
+  __syncthreads();
 }
 
 __global__ void __launch_bounds__(HQ_THREADS, 1)
 k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int b, int resident) {
   extern __shared__ __align__(16) double smem[];
   __shared__ HqChain ch;
-  __shared__ double tau_s;
   const int c = blockIdx.x;
   if (c >= nchains) return;
   if (threadIdx.x == 0) ch = chains[c];
@@ -707,99 +780,89 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
   if (!ch.active || b >= ch.n_stab) return;
   const int N = ch.N;
   const int entry = b;  // push position: the pushing stack holds b entries
+  const int ldp = panel_ld(N);
   double* A;
   int ld;
   double* p = smem;
-  if (resident) { A = p; ld = smem_ld(N); p += (size_t)N * ld; copy_mat(A, ld, ch.X, N, N); }
-  else { A = ch.X; ld = N; }
-  double* vn1 = p; p += N;
-  double* vn2 = p; p += N;
+  if (resident) { A = p; ld = smem_ld(N); p += (size_t)N * ld; }
+  else { A = ch.W3; ld = N; }  // W3 is free during a push
+  double* Vb = p; p += (size_t)ldp * kQB;
+  double* W = p; p += (size_t)kQB * ldp;
+  double* T = p; p += kQB * kQB;
+  double* S = p; p += kQB * kQB;
   double* tau = p; p += N;
-  double* wv = p; p += N;
-  int* jpvt = reinterpret_cast<int*>(p);
+  double* nrm = p; p += N;
+  int* order = reinterpret_cast<int*>(p);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  __syncthreads();
+  const double* X = ch.X;
+  // ---- pre-pivoting: columns by decreasing norm (ties by index) ----
   for (int j = warp; j < N; j += nwarps) {
     double s2 = 0.0;
-    for (int i = lane; i < N; i += 32) { const double v = A[i + (size_t)j * ld]; s2 = fma(v, v, s2); }
+    for (int i = lane; i < N; i += 32) { const double v = X[i + (size_t)j * N]; s2 = fma(v, v, s2); }
     s2 = warp_sum(s2);
-    if (lane == 0) { vn1[j] = sqrt(s2); vn2[j] = vn1[j]; jpvt[j] = j; }
+    if (lane == 0) nrm[j] = s2;
   }
   __syncthreads();
-  for (int i = 0; i < N; ++i) {
-    if (warp == 0) {
-      // pivot: first maximum of vn1[i:N] (idamax)
-      double best = -1.0;
-      int bi = i;
-      for (int j = i + lane; j < N; j += 32) {
-        const double v = vn1[j];
-        if (v > best) { best = v; bi = j; }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-      }
-      if (bi != i) {
-        for (int r = lane; r < N; r += 32) {
-          const double t0 = A[r + (size_t)bi * ld];
-          A[r + (size_t)bi * ld] = A[r + (size_t)i * ld];
-          A[r + (size_t)i * ld] = t0;
-        }
-        if (lane == 0) {
-          const int tj = jpvt[bi]; jpvt[bi] = jpvt[i]; jpvt[i] = tj;
-          vn1[bi] = vn1[i];
-          vn2[bi] = vn2[i];
-        }
-      }
-      __syncwarp();
-      // reflector of A[i:N, i] (dlarfg)
-      double xs = 0.0;
-      for (int r = i + 1 + lane; r < N; r += 32) { const double v = A[r + (size_t)i * ld]; xs = fma(v, v, xs); }
-      xs = warp_sum(xs);
-      const double alpha = A[i + (size_t)i * ld];
-      double ti = 0.0, beta = alpha;
-      if (xs > 0.0) {
-        beta = -copysign(hypot(alpha, sqrt(xs)), alpha);
-        ti = (beta - alpha) / beta;
-        const double sc = 1.0 / (alpha - beta);
-        for (int r = i + 1 + lane; r < N; r += 32) A[r + (size_t)i * ld] *= sc;
-      }
-      __syncwarp();
-      if (lane == 0) { A[i + (size_t)i * ld] = beta; tau[i] = ti; tau_s = ti; }
+  for (int j = threadIdx.x; j < N; j += blockDim.x) {
+    const double nj = nrm[j];
+    int rank = 0;
+    for (int i = 0; i < N; ++i) {
+      const double ni = nrm[i];
+      rank += (ni > nj || (ni == nj && i < j)) ? 1 : 0;
     }
-    __syncthreads();
-    // apply H(i) = I - tau v v^T to A[i:N, i+1:N] (v_i = 1) and downdate the norms
-    householder_trailing(A, ld, N, i, tau_s, vn1, vn2, true, true);
-    __syncthreads();
+    order[rank] = j;
   }
-  // D = |diag R| and T = D^-1 R P^T  (T[:, jpvt[c]] = row-scaled R[:, c])
+  __syncthreads();
+  HQ_FOR_EACH_ELEM(N, i, j) A[i + (size_t)j * ld] = X[i + (size_t)order[j] * N];
+  __syncthreads();
+  // ---- blocked Householder QR ----
+  for (int p0 = 0; p0 < N; p0 += kQB) {
+    const int p1 = min(p0 + kQB, N);
+    qr_panel(A, ld, N, p0, p1, tau);
+    if (p1 < N) {
+      wy_factor(A, ld, N, p0, p1 - p0, tau, Vb, ldp, T, S);
+      wy_apply(A, ld, N, p0, Vb, ldp, T, true, W, ldp, p1, N - p1);
+    }
+  }
+  // ---- D = |diag R|, T = D^-1 R P^T (T[:, order[c]] = row-scaled R[:, c]) ----
   const size_t NN = (size_t)N * N;
   double* Dout = ch.stackD + ((size_t)side * ch.n_stab + entry) * N;
-  double* T = ch.W0;
+  double* Tout = ch.W0;
   for (int r = threadIdx.x; r < N; r += blockDim.x) {
     const double dr = fabs(A[r + (size_t)r * ld]);
     Dout[r] = dr;
-    wv[r] = dr;
+    nrm[r] = dr;
   }
   __syncthreads();
   HQ_FOR_EACH_ELEM(N, r, cc) {
-    const double v = (r <= cc) ? A[r + (size_t)cc * ld] / wv[r] : 0.0;
-    T[r + (size_t)jpvt[cc] * N] = (wv[r] != 0.0) ? v : (r == cc ? 1.0 : 0.0);
+    const double v = (r <= cc) ? A[r + (size_t)cc * ld] / nrm[r] : 0.0;
+    Tout[r + (size_t)order[cc] * N] = (nrm[r] != 0.0) ? v : (r == cc ? 1.0 : 0.0);
   }
   __syncthreads();
-  // form Q in place from the reflectors (dorg2r): i = N-1 .. 0
-  for (int i = N - 1; i >= 0; --i) {
-    const double ti = tau[i];
-    if (i < N - 1) {
-      householder_trailing(A, ld, N, i, ti, vn1, vn2, false, true);
+  // ---- form Q in place, panels backwards ----
+  for (int p0 = ((N - 1) / kQB) * kQB; p0 >= 0; p0 -= kQB) {
+    const int p1 = min(p0 + kQB, N);
+    if (p1 < N) {
+      wy_factor(A, ld, N, p0, p1 - p0, tau, Vb, ldp, T, S);
+      wy_apply(A, ld, N, p0, Vb, ldp, T, false, W, ldp, p1, N - p1);
+    }
+    // unblocked formation of the panel's own columns (dorg2r restricted to the panel)
+    for (int i = p1 - 1; i >= p0; --i) {
+      const double ti = tau[i];
+      const int j = i + 1 + warp;
+      if (ti != 0.0 && j < p1) {
+        double w = (lane == 0) ? A[i + (size_t)j * ld] : 0.0;
+        for (int r = i + 1 + lane; r < N; r += 32) w = fma(A[r + (size_t)i * ld], A[r + (size_t)j * ld], w);
+        w = warp_sum(w) * ti;
+        if (lane == 0) A[i + (size_t)j * ld] -= w;
+        for (int r = i + 1 + lane; r < N; r += 32) A[r + (size_t)j * ld] = fma(-w, A[r + (size_t)i * ld], A[r + (size_t)j * ld]);
+      }
       __syncthreads();
       for (int r = i + 1 + threadIdx.x; r < N; r += blockDim.x) A[r + (size_t)i * ld] *= -ti;
+      if (threadIdx.x == 0) A[i + (size_t)i * ld] = 1.0 - ti;
+      for (int r = threadIdx.x; r < i; r += blockDim.x) A[r + (size_t)i * ld] = 0.0;
+      __syncthreads();
     }
-    if (threadIdx.x == 0) A[i + (size_t)i * ld] = 1.0 - ti;
-    for (int r = threadIdx.x; r < i; r += blockDim.x) A[r + (size_t)i * ld] = 0.0;
-    __syncthreads();
   }
   double* Uout = ch.stackU + ((size_t)side * ch.n_stab + entry) * NN;
   copy_mat(Uout, N, A, ld, N);
@@ -807,16 +870,23 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
 
 // ---------------------------------------------------------------------------------
 //  k_invert: in-place Gauss-Jordan inverse with partial (row) pivoting of the N x N
-//  matrix at `which` (0: W1, 1: W2, 2: W3, 3: W5). Two barriers per pivot: warp 0 finds
-//  the pivot and stages the scaled pivot row (prow) and the old row k (krow); then every
-//  warp eliminates its own rows. The row interchanges are undone as one column gather on
-//  the way out. Failure (zero pivot / non-finite) sets acc[STATUS].
+//  matrix at `which` (0: W1, 1: W2, 2: W3, 3: W5), blocked by panels of kGJ pivots.
+//
+//  Unblocked Gauss-Jordan reads and writes the whole matrix at every pivot, which in
+//  shared memory costs ~N^3/8 cycles. Here the pivots of a panel are applied to the
+//  panel's own columns only (one thread per row); their composition acts on every other
+//  column j as  A[:, j] += (P - E_K) A[K, j]  (P: the panel columns afterwards, K: the
+//  panel's pivot rows, E_K: their identity columns), a rank-kGJ update done with the DMMA
+//  flush of the Metropolis panels. The row interchanges of a panel are applied to the
+//  other columns before that update; the column interchanges that undo them are a
+//  gather on the way out. Failure (zero pivot / non-finite) sets acc[STATUS].
 // ---------------------------------------------------------------------------------
+constexpr int kGJ = 16;
+
 __global__ void __launch_bounds__(HQ_THREADS, 1)
 k_invert(const HqChain* __restrict__ chains, int nchains, int b, int which, int resident) {
   extern __shared__ __align__(16) double smem[];
   __shared__ HqChain ch;
-  __shared__ int piv_s;
   const int c = blockIdx.x;
   if (c >= nchains) return;
   if (threadIdx.x == 0) ch = chains[c];
@@ -829,54 +899,86 @@ k_invert(const HqChain* __restrict__ chains, int nchains, int b, int which, int 
   double* p = smem;
   if (resident) { A = p; ld = smem_ld(N); p += (size_t)N * ld; copy_mat(A, ld, src, N, N); }
   else { A = src; ld = N; }
-  double* prow = p; p += N;
-  double* krow = p; p += N;
+  const int ldp = panel_ld(N);
+  double* Wp = p; p += (size_t)ldp * kGJ;   // N x kGJ, column-major
+  double* Bf = p; p += (size_t)ldp * kGJ;   // kGJ x N, row-major
   int* perm = reinterpret_cast<int*>(p);
   int* gidx = perm + N;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __syncthreads();
-  for (int k = 0; k < N; ++k) {
-    if (warp == 0) {
-      double best = -1.0;
-      int bi = k;
-      for (int r = k + lane; r < N; r += 32) {
-        const double v = fabs(A[r + (size_t)k * ld]);
-        if (v > best) { best = v; bi = r; }
-      }
+  for (int p0 = 0; p0 < N; p0 += kGJ) {
+    const int nb = min(kGJ, N - p0);
+    for (int q = 0; q < nb; ++q) {
+      const int k = p0 + q;
+      if (warp == 0) {
+        // pivot search in column k over rows k..N-1, swap within the panel, scale the pivot row
+        double best = -1.0;
+        int bi = k;
+        for (int r = k + lane; r < N; r += 32) {
+          const double v = fabs(A[r + (size_t)k * ld]);
+          if (v > best) { best = v; bi = r; }
+        }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        const bool ok = (best > 0.0) && isfinite(best);
+        if (lane < nb && bi != k) {
+          const int j = p0 + lane;
+          const double t0 = A[k + (size_t)j * ld];
+          A[k + (size_t)j * ld] = A[bi + (size_t)j * ld];
+          A[bi + (size_t)j * ld] = t0;
+        }
+        __syncwarp();
+        const double pv = A[k + (size_t)k * ld];
+        const double pinv = ok ? 1.0 / pv : 0.0;
+        __syncwarp();
+        if (lane < nb) {
+          const int j = p0 + lane;
+          const double v = (j == k) ? 1.0 : A[k + (size_t)j * ld];
+          A[k + (size_t)j * ld] = v * pinv;
+        }
+        if (lane == 0) {
+          perm[k] = bi;
+          if (!ok) ch.acc[HQ_ACC_STATUS] = 1.0;
+        }
       }
-      const double pval = A[bi + (size_t)k * ld];
-      const bool ok = (best > 0.0) && isfinite(best);
-      const double pinv = ok ? 1.0 / pval : 0.0;
-      for (int j = lane; j < N; j += 32) {
-        krow[j] = A[k + (size_t)j * ld];
-        prow[j] = (j == k ? 1.0 : A[bi + (size_t)j * ld]) * pinv;
+      __syncthreads();
+      // eliminate column k from every other row of the panel (one thread per row)
+      for (int r = threadIdx.x; r < N; r += blockDim.x) {
+        if (r == k) continue;
+        const double f = A[r + (size_t)k * ld];
+#pragma unroll 4
+        for (int jj = 0; jj < nb; ++jj) {
+          const int j = p0 + jj;
+          const double base = (j == k) ? 0.0 : A[r + (size_t)j * ld];
+          A[r + (size_t)j * ld] = fma(-f, A[k + (size_t)j * ld], base);
+        }
       }
-      if (lane == 0) {
-        perm[k] = bi;
-        piv_s = bi;
-        if (!ok) ch.acc[HQ_ACC_STATUS] = 1.0;
-      }
+      __syncthreads();
     }
+    // rows interchanges of this panel on every other column, then the pivot rows into Bf
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+      const bool in_panel = (j >= p0 && j < p0 + nb);
+      if (!in_panel) {
+        for (int q = 0; q < nb; ++q) {
+          const int k = p0 + q, pr = perm[k];
+          if (pr != k) {
+            const double t0 = A[k + (size_t)j * ld];
+            A[k + (size_t)j * ld] = A[pr + (size_t)j * ld];
+            A[pr + (size_t)j * ld] = t0;
+          }
+        }
+      }
+      for (int q = 0; q < nb; ++q) Bf[q * ldp + j] = in_panel ? 0.0 : A[p0 + q + (size_t)j * ld];
+    }
+    for (int r = threadIdx.x; r < N; r += blockDim.x)
+      for (int q = 0; q < nb; ++q) Wp[r + q * ldp] = A[r + (size_t)(p0 + q) * ld] - (r == p0 + q ? 1.0 : 0.0);
     __syncthreads();
-    const int pr = piv_s;
-    for (int r = warp; r < N; r += nwarps) {
-      if (r == k) {
-        for (int j = lane; j < N; j += 32) A[k + (size_t)j * ld] = prow[j];
-        continue;
-      }
-      const bool from_k = (r == pr);
-      const double f = from_k ? krow[k] : A[r + (size_t)k * ld];
-      __syncwarp();
-      for (int j = lane; j < N; j += 32) {
-        const double s0 = from_k ? krow[j] : A[r + (size_t)j * ld];
-        A[r + (size_t)j * ld] = fma(-f, prow[j], (j == k) ? 0.0 : s0);
-      }
-    }
+    // A[:, j] += Wp Bf[:, j] for every column outside the panel (Bf is zero on the panel)
+    flush_panels(A, ld, N, Wp, ldp, Bf, ldp, nb);
     __syncthreads();
   }
   // undo the row interchanges as column interchanges in reverse order: column j of the
@@ -891,7 +993,6 @@ k_invert(const HqChain* __restrict__ chains, int nchains, int b, int which, int 
   if (resident) {
     HQ_FOR_EACH_ELEM(N, i, j) src[i + (size_t)j * N] = A[i + (size_t)gidx[j] * ld];
   } else {
-    // in global memory: apply the interchanges one by one
     for (int k = N - 1; k >= 0; --k) {
       const int q = perm[k];
       if (q != k)
@@ -1320,6 +1421,12 @@ namespace hq {
 size_t smem_interval_bytes(int Nmax, int kmax, bool resident) {
   return interval_smem_doubles(Nmax, kmax, resident) * sizeof(double);
 }
+size_t smem_udt_bytes(int Nmax, bool resident) {
+  return smem_matrix_bytes(Nmax, resident, 2 * kQB * panel_ld(Nmax) + 2 * kQB * kQB + 3 * Nmax + 64);
+}
+size_t smem_invert_bytes(int Nmax, bool resident) {
+  return smem_matrix_bytes(Nmax, resident, 2 * kGJ * panel_ld(Nmax) + Nmax + 64);
+}
 size_t smem_matrix_bytes(int Nmax, bool resident, int extra_doubles) {
   const size_t mat = resident ? (size_t)Nmax * smem_ld(Nmax) : 0;
   return (mat + (size_t)extra_doubles) * sizeof(double);
@@ -1350,8 +1457,8 @@ cudaError_t prepare_kernels(int Nmax, int kmax, bool resident) {
   cudaError_t e;
   if ((e = raise_smem(0, (const void*)k_interval, smem_interval_bytes(Nmax, kmax, resident))) != cudaSuccess) return e;
   if ((e = raise_smem(1, (const void*)k_bchain, mat_stage)) != cudaSuccess) return e;
-  if ((e = raise_smem(2, (const void*)k_udt, smem_matrix_bytes(Nmax, resident, 5 * Nmax + 64))) != cudaSuccess) return e;
-  if ((e = raise_smem(3, (const void*)k_invert, smem_matrix_bytes(Nmax, resident, 3 * Nmax + 64))) != cudaSuccess) return e;
+  if ((e = raise_smem(2, (const void*)k_udt, smem_udt_bytes(Nmax, resident))) != cudaSuccess) return e;
+  if ((e = raise_smem(3, (const void*)k_invert, smem_invert_bytes(Nmax, resident))) != cudaSuccess) return e;
   if ((e = raise_smem(4, (const void*)k_dyn_slices, mat_stage)) != cudaSuccess) return e;
   if ((e = raise_smem(5, (const void*)k_adj_interval, mat_stage)) != cudaSuccess) return e;
   return cudaSuccess;
@@ -1369,12 +1476,12 @@ cudaError_t launch_bchain(const HqChain* chains, int n, int dir, int b, int Nmax
   return cudaGetLastError();
 }
 cudaError_t launch_udt(const HqChain* chains, int n, int side, int b, int Nmax, bool resident, cudaStream_t st) {
-  const size_t bytes = smem_matrix_bytes(Nmax, resident, 5 * Nmax + 64);
+  const size_t bytes = smem_udt_bytes(Nmax, resident);
   k_udt<<<n, HQ_THREADS, bytes, st>>>(chains, n, side, 0, b, resident ? 1 : 0);
   return cudaGetLastError();
 }
 cudaError_t launch_invert(const HqChain* chains, int n, int b, int which, int Nmax, bool resident, cudaStream_t st) {
-  const size_t bytes = smem_matrix_bytes(Nmax, resident, 3 * Nmax + 64);
+  const size_t bytes = smem_invert_bytes(Nmax, resident);
   k_invert<<<n, HQ_THREADS, bytes, st>>>(chains, n, b, which, resident ? 1 : 0);
   return cudaGetLastError();
 }

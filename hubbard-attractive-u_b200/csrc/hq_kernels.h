@@ -7,6 +7,8 @@
 namespace hq {
 size_t smem_interval_bytes(int Nmax, int kmax, bool resident);
 size_t smem_matrix_bytes(int Nmax, bool resident, int extra_doubles);
+size_t smem_invert_bytes(int Nmax, bool resident);
+size_t smem_udt_bytes(int Nmax, bool resident);
 cudaError_t prepare_kernels(int Nmax, int kmax, bool resident);
 cudaError_t launch_interval(const HqChain* chains, int n, int dir, int b, int flags, int Nmax, int kmax, bool resident,
                             cudaStream_t st);

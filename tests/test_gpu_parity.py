@@ -1,12 +1,13 @@
 """GPU parity tests: the sm_100a sweep through the C ABI against the CPU oracle.
 
 Tolerances (FP64):
-  * G(tau,tau), G(tau,0), G(0,tau): max-abs <= 1e-10 wherever the reference algorithm
-    itself is accurate to that level (small and moderate beta); at large beta the
-    oracle's own wrap error bounds what a second implementation can agree to, and the
-    check is against max(1e-10, 10 x that error) plus a pace-1 comparison at 1e-10.
-  * acceptance ratios of the replayed random stream: relative 1e-10 (median 1e-13; the
-    ratio amplifies the G difference of wrapped slices ~3.5x);
+  * G(tau,tau), G(tau,0), G(0,tau): max-abs <= 1e-10 on freshly stabilised slices; on
+    wrapped slices each implementation drifts from the exact G by up to its own wrap error
+    (the quantity the reference reports), so the bound there is max(1e-10, 2 x (sum of
+    both wrap errors)) -- at large beta 10 x the oracle's -- plus a pace-1 comparison
+    at 1e-10 relative to max|G|.
+  * acceptance ratios of the replayed random stream: median relative 1e-13; max within
+    the G bound of wrapped slices times |dr/dG_ii| (~3.5);
   * Ising fields and acceptance counts: identical.
 """
 import math
@@ -39,16 +40,31 @@ def test_c1_sweeps_all_slices(hq, oracle, mode):
     assert np.abs(e.g(0) - o.g()).max() <= 1e-10
     for _ in range(2):
         for d in (UP, DOWN):
+            e.reset_estimators(reset_wrap=True)
             e.sweep(d, hq.SWEEP_MEASURE | hq.SWEEP_SNAPSHOT)
             o.sweep(d)
             assert np.array_equal(e.fields(0), o.fields())
-            errs = [np.abs(e.g(0, hq.G_TT, t) - o.g_slice(0, t)).max() for t in range(40)]
-            assert max(errs) <= 1e-10, max(errs)
+            errs = np.array([np.abs(e.g(0, hq.G_TT, t) - o.g_slice(0, t)).max() for t in range(40)])
+            # freshly stabilised slices (tau = 0, 10, 20, 30): 1e-10 outright
+            assert errs[::10].max() <= 1e-10, errs[::10].max()
+            # wrapped slices: each implementation drifts from the exact G by up to its wrap
+            # error (the reference reports the same quantity); the difference is bounded by both
+            floor = max(1e-10, 2.0 * (e.wrap_errors(0)[0] + o.wrap_errors()[0]))
+            assert errs.max() <= floor, (errs.max(), floor)
+    wt, _ = e.wrap_errors(0)
+    assert 0.0 <= wt < 1e-8
+    e.close()
+
+
+def test_c1_acceptance_counts(hq, oracle):
+    e, o = pair(hq, oracle)
+    for _ in range(2):
+        for d in (UP, DOWN):
+            e.sweep(d, hq.SWEEP_MEASURE)
+            o.sweep(d)
     est = e.estimators(0)
     cnt = o.counts()
     assert est[4] == cnt[0] and est[5] == cnt[1]
-    wt, _ = e.wrap_errors(0)
-    assert 0.0 <= wt < 1e-8
     e.close()
 
 
@@ -64,10 +80,11 @@ def test_ratio_replay(hq, oracle):
     ro = o.ratios()
     assert len(rg) == len(ro) == cap
     rel = np.abs(rg - ro) / np.maximum(1.0, np.abs(ro))
-    # r = a^2 / (1 + Delta) carries |dr/dG_ii| ~ 3.5 x the G difference, and wrapped G's of
-    # two implementations differ by up to ~2e-11 here (the wrap rounding the reference
-    # reports as its wrap error): right after a stabilisation the ratios agree to ~1e-14
-    assert rel.max() <= 1e-10, rel.max()
+    # r = a^2 / (1 + Delta) carries |dr/dG_ii| ~ 3.5 x the G difference; wrapped G's of two
+    # implementations differ by up to the sum of their wrap errors (the wrap rounding the
+    # reference reports), and right after a stabilisation the ratios agree to ~1e-14
+    bound = max(1e-10, 4.0 * 2.0 * (e.wrap_errors(0)[0] + o.wrap_errors()[0]))
+    assert rel.max() <= bound, (rel.max(), bound)
     assert np.median(rel) <= 1e-13, np.median(rel)
     assert np.array_equal(e.fields(0), o.fields())
     e.close()
