@@ -148,13 +148,17 @@ __device__ inline void sep_pass(double* M, int ld, int N, const double* __restri
     double v[L];
 #pragma unroll
     for (int e = 0; e < L; ++e) v[e] = base[e * stride];
+    // L independent accumulators, each summed over e2 in ascending order
+    double acc[L];
 #pragma unroll
-    for (int e = 0; e < L; ++e) {
-      double acc = 0.0;
+    for (int e = 0; e < L; ++e) acc[e] = 0.0;
 #pragma unroll
-      for (int e2 = 0; e2 < L; ++e2) acc = fma(a[(e - e2 + L) % L], v[e2], acc);
-      base[e * stride] = (pass == 1) ? acc * c : acc;
+    for (int e2 = 0; e2 < L; ++e2) {
+#pragma unroll
+      for (int e = 0; e < L; ++e) acc[e] = fma(a[(e - e2 + L) % L], v[e2], acc[e]);
     }
+#pragma unroll
+    for (int e = 0; e < L; ++e) base[e * stride] = (pass == 1) ? acc[e] * c : acc[e];
   }
 }
 

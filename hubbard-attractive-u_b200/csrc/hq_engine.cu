@@ -491,7 +491,7 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   // ---- delay depth and shared-memory residency ----
   int smem_optin = 0;
   HQ_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
-  const size_t budget = size_t(smem_optin) - 4096;  // static shared memory of the kernels
+  const size_t budget = size_t(smem_optin) - hq::max_static_smem();
   c->resident = hq::smem_interval_bytes(c->Nmax, 4, true) <= budget &&
                 hq::smem_matrix_bytes(c->Nmax, true, 8 * (((c->Nmax + 15) & ~15) + 4) + 64) <= budget &&
                 hq::smem_invert_bytes(c->Nmax, true) <= budget && hq::smem_udt_bytes(c->Nmax, true) <= budget;
@@ -500,8 +500,9 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
     if (hq::smem_interval_bytes(c->Nmax, k, c->resident) <= budget) { kfit = k; break; }
   for (int i = 0; i < n_chains; ++i) {
     ChainHost& h = c->ch[i];
-    h.kmax = h.p.delay_depth > 0 ? std::min(h.p.delay_depth, kfit) : kfit;
-    h.kmax = std::max(1, h.kmax);
+    // the delay depth is the site-block size of the submatrix updates: 4, 8 or 16
+    const int want = h.p.delay_depth > 0 ? std::min(h.p.delay_depth, kfit) : kfit;
+    h.kmax = want >= 16 ? 16 : (want >= 8 ? 8 : 4);
     c->kmax_max = std::max(c->kmax_max, h.kmax);
   }
   if (hq::smem_interval_bytes(c->Nmax, c->kmax_max, c->resident) > budget)

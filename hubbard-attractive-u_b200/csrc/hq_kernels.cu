@@ -33,10 +33,15 @@ __host__ __device__ inline int smem_ld(int N) { return (N % 2 == 0) ? N + 1 : N;
 // fragment loads of the flush are free of bank conflicts
 __host__ __device__ inline int panel_ld(int N) { return N + ((4 - N % 16) + 16) % 16; }
 
-// bytes of dynamic shared memory of k_interval / k_bchain for a chain of size N with
-// delay depth kmax (matrix in smem when `resident`)
+// leading dimension of the resident G of k_interval: = 2 (mod 8) doubles, so that the DMMA
+// accumulator tiles of the rank updates (lane 4g+q at row g, columns 2q, 2q+1) are free of
+// bank conflicts
+__host__ __device__ inline int interval_ld(int N) { return N + ((2 - N % 8) + 8) % 8; }
+
+// bytes of dynamic shared memory of k_interval for a chain of size N with delay depth kmax
+// (matrix in smem when `resident`)
 __host__ __device__ inline size_t interval_smem_doubles(int N, int kmax, bool resident) {
-  const size_t mat = resident ? (size_t)N * smem_ld(N) : 0;
+  const size_t mat = resident ? (size_t)N * interval_ld(N) : 0;
   const size_t panels = (size_t)panel_ld(N) * kmax * 2;
   const size_t stage = (size_t)8 * (((N + 15) & ~15) + 4);
   const size_t work = panels > stage ? panels : stage;
@@ -73,57 +78,95 @@ __device__ void copy_mat(double* dst, int ldd, const double* src, int lds, int N
 }
 
 // ---------------------------------------------------------------------------------
-//  Metropolis sweep over the N sites of one slice with delayed rank-k updates.
+//  Metropolis sweep over the N sites of one slice: submatrix (block-delayed) updates.
 //
 //  The reference visits i = 0..N-1 in order, draws one uniform per site, and on
 //  acceptance applies G -= gamma G[:,i] (e_i^T - G[i,:]), gamma = Delta/(1+(1-G_ii)Delta)
-//  (src/hubbard.cpp:123-139). A rejected site leaves G unchanged, so the ratio of every
-//  later site only depends on the current diagonal: all remaining sites are tested in
-//  parallel and the first acceptance is taken, then the search resumes after it. The
-//  accepted updates are kept as G = G0 + X Y (X: N x k, Y: k x N) and flushed into G0
-//  with DMMA when k reaches kmax and at the end of the slice.
+//  (src/hubbard.cpp:123-139). Here the sites are taken in blocks J of NB consecutive
+//  sites (E. Gull, P. Staar, S. Fuchs et al., Submatrix updates for the continuous-time
+//  auxiliary-field algorithm, Phys. Rev. B 83, 075122 (2011), applied to the Ising HS
+//  field):
+//   1. the walk: one warp holds g = G[J, J] in registers and visits the NB sites in order
+//      with the reference's acceptance test and rank-1 updates of g alone (every later
+//      decision of the block reads only g's diagonal). For the a accepted flips
+//      j_0 < j_1 < ... it records gamma_m, X[J, m] = gamma_m g[:, j_m] and
+//      Y[m, J] = g[j_m, :] - e_{j_m}^T (g before flip m);
+//   2. the sequential updates compose to G_new = G + X Y with
+//        X = G[:, Ja] Gamma (I - C Gamma)^-1,   C[m', m] = Y[m', j_m]  (strictly upper)
+//        Y = (I - D)^-1 (G[Ja, :] - E),         D[m, m'] = X[j_m, m']  (strictly lower)
+//      the walking warp forms the two a x a unit-triangular inverses from its records,
+//      and X, Y are two small DMMA products over all warps;
+//   3. G += X Y by DMMA (rank a <= NB). While warps 1.. flush block b, warp 0 applies
+//      the same update to the next block's diagonal tile G[J', J'] (which the flush
+//      skips) and walks block b+1.
+//  The result equals the reference's sequence of rank-1 updates up to rounding.
 // ---------------------------------------------------------------------------------
-// G[0:M, 0:Nc] += X[0:M, 0:k] Y[0:k, 0:Nc]  (X column-major ldx, Y row-major ldy), by 16 x 32
-// strips of four 16 x 8 DMMA tiles that share the A fragments
-__device__ void rank_update(double* G, int ld, int M, int Nc, const double* X, int ldx, const double* Y, int ldy,
-                            int k) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+// G[0:M, 0:Nc] += X[0:M, 0:k] Y[0:k, 0:Nc]  (X column-major ldx, Y row-major ldy, k <= 16),
+// by 16 x 32 strips of four 16 x 8 DMMA tiles that share the A fragments; the fragments of
+// all k-steps are loaded before the strip's G tiles so that their latencies overlap.
+// Warps w0 .. w0+nw-1 take part; elements with both indices in [ex0, ex1) are left alone.
+__device__ void rank_update_ex(double* G, int ld, int M, int Nc, const double* X, int ldx, const double* Y,
+                               int ldy, int k, int w0, int nw, int ex0, int ex1) {
+  const int lane = threadIdx.x & 31, warp = (threadIdx.x >> 5) - w0;
   const int g = lane >> 2, q = lane & 3;
   const int mt = (M + 15) / 16, ns = (Nc + 31) / 32;
   const int strips = mt * ns;
-  for (int st = warp; st < strips; st += nwarps) {
+  const int ksteps = (k + 3) >> 2;  // <= 4
+  for (int st = warp; st < strips; st += nw) {
     const int r0 = (st % mt) * 16, c0 = (st / mt) * 32;
     const int r = r0 + g;
-    double acc[4][4];
+    double fa0[4], fa1[4], fb[4][4];
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int c = c0 + t * 8 + 2 * q;
-      acc[t][0] = (r < M && c < Nc) ? G[r + (size_t)c * ld] : 0.0;
-      acc[t][1] = (r < M && c + 1 < Nc) ? G[r + (size_t)(c + 1) * ld] : 0.0;
-      acc[t][2] = (r + 8 < M && c < Nc) ? G[r + 8 + (size_t)c * ld] : 0.0;
-      acc[t][3] = (r + 8 < M && c + 1 < Nc) ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
-    }
-    for (int m0 = 0; m0 < k; m0 += 4) {
-      const int m = m0 + q;
-      const bool mk = m < k;
-      const double a0 = (r < M && mk) ? X[r + m * ldx] : 0.0;
-      const double a1 = (r + 8 < M && mk) ? X[r + 8 + m * ldx] : 0.0;
+    for (int s = 0; s < 4; ++s) {
+      const int m = 4 * s + q;
+      const bool mk = s < ksteps && m < k;
+      fa0[s] = (r < M && mk) ? X[r + m * ldx] : 0.0;
+      fa1[s] = (r + 8 < M && mk) ? X[r + 8 + m * ldx] : 0.0;
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int cb = c0 + t * 8 + g;
-        const double b0 = (cb < Nc && mk) ? Y[m * ldy + cb] : 0.0;
-        dmma_16x8x4(acc[t], a0, a1, b0);
+        fb[s][t] = (cb < Nc && mk) ? Y[m * ldy + cb] : 0.0;
+      }
+    }
+    // element masks: in range and outside the excluded tile
+    const bool rin0 = r < M && !(r >= ex0 && r < ex1), rin1 = r + 8 < M && !(r + 8 >= ex0 && r + 8 < ex1);
+    const bool rok0 = r < M, rok1 = r + 8 < M;
+    double acc[4][4];
+    bool w[4][4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int c = c0 + t * 8 + 2 * q;
+      const bool cx0 = c >= ex0 && c < ex1, cx1 = c + 1 >= ex0 && c + 1 < ex1;
+      w[t][0] = rok0 && c < Nc && (rin0 || !cx0);
+      w[t][1] = rok0 && c + 1 < Nc && (rin0 || !cx1);
+      w[t][2] = rok1 && c < Nc && (rin1 || !cx0);
+      w[t][3] = rok1 && c + 1 < Nc && (rin1 || !cx1);
+      acc[t][0] = w[t][0] ? G[r + (size_t)c * ld] : 0.0;
+      acc[t][1] = w[t][1] ? G[r + (size_t)(c + 1) * ld] : 0.0;
+      acc[t][2] = w[t][2] ? G[r + 8 + (size_t)c * ld] : 0.0;
+      acc[t][3] = w[t][3] ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      if (s < ksteps) {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) dmma_16x8x4(acc[t], fa0[s], fa1[s], fb[s][t]);
       }
     }
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       const int c = c0 + t * 8 + 2 * q;
-      if (r < M && c < Nc) G[r + (size_t)c * ld] = acc[t][0];
-      if (r < M && c + 1 < Nc) G[r + (size_t)(c + 1) * ld] = acc[t][1];
-      if (r + 8 < M && c < Nc) G[r + 8 + (size_t)c * ld] = acc[t][2];
-      if (r + 8 < M && c + 1 < Nc) G[r + 8 + (size_t)(c + 1) * ld] = acc[t][3];
+      if (w[t][0]) G[r + (size_t)c * ld] = acc[t][0];
+      if (w[t][1]) G[r + (size_t)(c + 1) * ld] = acc[t][1];
+      if (w[t][2]) G[r + 8 + (size_t)c * ld] = acc[t][2];
+      if (w[t][3]) G[r + 8 + (size_t)(c + 1) * ld] = acc[t][3];
     }
   }
+}
+
+__device__ void rank_update(double* G, int ld, int M, int Nc, const double* X, int ldx, const double* Y, int ldy,
+                            int k) {
+  rank_update_ex(G, ld, M, Nc, X, ldx, Y, ldy, k, 0, blockDim.x >> 5, 0, 0);
 }
 
 // G += X Y on the full N x N matrix (the flush of the delayed Metropolis panels)
@@ -131,332 +174,261 @@ __device__ void flush_panels(double* G, int ld, int N, const double* X, int ldx,
   rank_update(G, ld, N, N, X, ldx, Y, ldy, k);
 }
 
-// barrier of the decision team (warps 0-3 of the interval kernel)
-__device__ __forceinline__ void team_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
-
 struct MetroShared {
-  double* d;      // current diagonal [N]
+  double* dl;     // Delta of each site [N]
   double* u;      // uniforms [N]
-  double* rr;     // last ratio of each site [N] (ratio log)
+  double* rr;     // visit-time ratio of each site [N] (ratio log)
   int8_t* s;      // fields of the slice [N]
   int8_t* flip;   // accepted flags [N]
-  double* X;      // N x kmax
-  double* Y;      // kmax x N (row-major)
-  int* ired;      // >= 32 ints
-  int* qj;        // accepted site of each panel column [kmax]
-  double* qg;     // gamma of each panel column [kmax]
-  double* gam;    // speculative gamma of the sites of a search round [128]
-  volatile int* qn;    // panel columns published by the decision warp
-  volatile int* qdone; // decision phase of this panel finished
+  double* X;      // N x 16 panel (column-major, ld panel_ld(N))
+  double* Y;      // 16 x N panel (row-major, ld panel_ld(N))
+  double* xl;     // X[J, m] of the block: xl[m * NB + s]
+  double* yl;     // Y[m, J] of the block: yl[m * NB + s]
+  double* Am;     // Gamma (I - C Gamma)^-1, 16 x 16 row-major, zero outside a x a
+  double* Bm;     // (I - D)^-1, 16 x 16 row-major, zero outside a x a
+  int* ired;      // >= 8 ints
+  int* qj;        // accepted site of each panel column [16]
+  double* qg;     // gamma of each panel column [16]
 };
 
-__device__ void metropolis_slice(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
-                                 double& n_acc, int flags, long long log_base) {
-  const int N = ch.N, kmax = ch.kmax;
+// the walk of the block [b0, b0 + nb) by one warp (see above); writes the records, the
+// accepted count into ired[slot] and the two triangular factors
+template <int NB>
+__device__ void walk_block(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0, int nb,
+                           bool log, int slot, double& acc_count) {
+  constexpr int R = (NB * NB >= 32) ? NB * NB / 32 : 1;  // rows of g held by one lane
+  constexpr int H = NB / R;                              // lane groups (rows h*R .. h*R+R-1)
+  const int lane = threadIdx.x & 31;
+  // lane layout of g: lane le = h * NB + c holds g[h*R + i][c], i < R (lanes >= NB*H mirror)
+  const int le = lane % (NB * H), c = le % NB, h = le / NB;
+  const bool writer = lane < NB * H;
+  double r[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int row = h * R + i;
+    r[i] = (row < nb && c < nb) ? G[b0 + row + (size_t)(b0 + c) * ld] : 0.0;
+  }
+  // per-site constants of the block, loaded before the walk (the walk's shared-memory
+  // stores would otherwise order every later load behind them)
+  double dls[NB], thr[NB];
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    dls[s] = s < nb ? sh.dl[b0 + s] : 0.0;
+    thr[s] = s < nb ? sh.u[b0 + s] * (1.0 + dls[s]) : 0.0;
+  }
+  int a = 0;
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    if (s < nb) {
+      const int ss = s / R, si = s % R;  // g[s][*] is held by group ss at register si
+      // column s, row s and the diagonal entry of the current g; gamma is formed before
+      // the decision so that its division overlaps the test
+      const double dg = __shfl_sync(0xffffffffu, r[si], ss * NB + s);
+      double colr[R];
+#pragma unroll
+      for (int i = 0; i < R; ++i) colr[i] = __shfl_sync(0xffffffffu, r[i], h * NB + s);
+      const double yv = __shfl_sync(0xffffffffu, r[si], ss * NB + c) - (c == s ? 1.0 : 0.0);
+      const double dl = dls[s];
+      const double av = 1.0 + (1.0 - dg) * dl;
+      const double gam = dl / av;
+      if (log && lane == 0) sh.rr[b0 + s] = (av * av) / (1.0 + dl);
+      // accept iff u < min(1, |r|), r = a^2 / (1 + Delta), 1 + Delta = e^{-2 alpha s} > 0
+      if (thr[s] < av * av) {
+        double colv[R];
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          colv[i] = gam * colr[i];
+          r[i] = fma(colv[i], yv, r[i]);
+        }
+        if (writer && c == 0) {
+#pragma unroll
+          for (int i = 0; i < R; ++i) sh.xl[a * NB + h * R + i] = colv[i];
+        }
+        if (writer && h == 0) sh.yl[a * NB + c] = yv;
+        if (lane == 0) {
+          sh.qj[a] = b0 + s;
+          sh.qg[a] = gam;
+          sh.flip[b0 + s] = 1;
+        }
+        ++a;
+      }
+    }
+  }
+  if (lane == 0) sh.ired[slot] = a;
+  acc_count += (lane == 0) ? (double)a : 0.0;
+  __syncwarp();
+  // unit-triangular inverses: lanes 0-15 row r of T = (I - C Gamma)^-1 (then A = Gamma T),
+  // lanes 16-31 column r of B = (I - D)^-1; both follow V[m] = delta_rm + s_m sum_{m'<m}
+  // V[m'] coef[m'][m] with coef read from the walk's records
+  const int rr_ = lane & 15;
+  const bool aside = lane < 16;
+  const double* cf = aside ? sh.yl : sh.xl;
+  double V[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    V[m] = 0.0;
+    if (m < a) {
+      const int sj = sh.qj[m] - b0;
+      double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+      for (int m2 = 0; m2 + 1 < m; m2 += 2) {
+        s0 = fma(V[m2], cf[m2 * NB + sj], s0);
+        s1 = fma(V[m2 + 1], cf[(m2 + 1) * NB + sj], s1);
+      }
+      if (m & 1) s0 = fma(V[m - 1], cf[(m - 1) * NB + sj], s0);
+      V[m] = (m == rr_ ? 1.0 : 0.0) + (aside ? sh.qg[m] : 1.0) * (s0 + s1);
+    }
+  }
+  const double sc = (rr_ < a) ? (aside ? sh.qg[rr_] : 1.0) : 0.0;
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    if (aside) sh.Am[rr_ * 16 + m] = sc * V[m];
+    else sh.Bm[m * 16 + rr_] = sc * V[m];
+  }
+}
+
+// X = G[:, Ja] A (N x 16) and Y = B (G[Ja, :] - E) (16 x N) into the panels, all warps
+__device__ void form_panels(const double* G, int ld, int N, const MetroShared& sh, int ldp, int a) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int mt = (N + 15) / 16, ntx = a > 8 ? 2 : 1, nty = (N + 7) / 8;
+  const int ksteps = (a + 3) >> 2;
+  int jq[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) jq[s] = (4 * s + q < a) ? sh.qj[4 * s + q] : 0;
+  for (int ti = warp; ti < mt * ntx + nty; ti += nwarps) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (ti < mt * ntx) {
+      const int r = (ti % mt) * 16 + g, n0 = (ti / mt) * 8;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        if (s < ksteps) {
+          const bool mk = 4 * s + q < a;
+          const double a0 = (r < N && mk) ? G[r + (size_t)jq[s] * ld] : 0.0;
+          const double a1 = (r + 8 < N && mk) ? G[r + 8 + (size_t)jq[s] * ld] : 0.0;
+          const double b0 = sh.Am[(4 * s + q) * 16 + n0 + g];
+          dmma_16x8x4(acc, a0, a1, b0);
+        }
+      }
+      // the panels hold a <= delay depth columns / rows
+      const int cc = n0 + 2 * q;
+      if (r < N && cc < a) sh.X[r + cc * ldp] = acc[0];
+      if (r < N && cc + 1 < a) sh.X[r + (cc + 1) * ldp] = acc[1];
+      if (r + 8 < N && cc < a) sh.X[r + 8 + cc * ldp] = acc[2];
+      if (r + 8 < N && cc + 1 < a) sh.X[r + 8 + (cc + 1) * ldp] = acc[3];
+    } else {
+      const int n0 = (ti - mt * ntx) * 8, n = n0 + g;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        if (s < ksteps) {
+          const int m = 4 * s + q;
+          const double a0 = sh.Bm[g * 16 + m], a1 = sh.Bm[(g + 8) * 16 + m];
+          const double b0 = (n < N && m < a) ? G[jq[s] + (size_t)n * ld] - (n == jq[s] ? 1.0 : 0.0) : 0.0;
+          dmma_16x8x4(acc, a0, a1, b0);
+        }
+      }
+      const int cc = n0 + 2 * q;
+      if (cc < N && g < a) sh.Y[g * ldp + cc] = acc[0];
+      if (cc + 1 < N && g < a) sh.Y[g * ldp + cc + 1] = acc[1];
+      if (cc < N && g + 8 < a) sh.Y[(g + 8) * ldp + cc] = acc[2];
+      if (cc + 1 < N && g + 8 < a) sh.Y[(g + 8) * ldp + cc + 1] = acc[3];
+    }
+  }
+}
+
+// warp 0: G[J', J'] += X[J', :] Y[:, J'] for the next block J' = [b0, b0 + nb) (nb <= 16)
+__device__ void correct_block(double* G, int ld, const MetroShared& sh, int ldp, int b0, int nb, int a) {
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2, q = lane & 3;
+  const int ksteps = (a + 3) >> 2;
+#pragma unroll
+  for (int tn = 0; tn < 2; ++tn) {
+    if (tn * 8 < nb) {
+      double acc[4];
+      const int c = tn * 8 + 2 * q;
+      const bool v00 = g < nb && c < nb, v01 = g < nb && c + 1 < nb;
+      const bool v10 = g + 8 < nb && c < nb, v11 = g + 8 < nb && c + 1 < nb;
+      acc[0] = v00 ? G[b0 + g + (size_t)(b0 + c) * ld] : 0.0;
+      acc[1] = v01 ? G[b0 + g + (size_t)(b0 + c + 1) * ld] : 0.0;
+      acc[2] = v10 ? G[b0 + g + 8 + (size_t)(b0 + c) * ld] : 0.0;
+      acc[3] = v11 ? G[b0 + g + 8 + (size_t)(b0 + c + 1) * ld] : 0.0;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        if (s < ksteps) {
+          const int m = 4 * s + q;
+          const bool mk = m < a;
+          const double a0 = (g < nb && mk) ? sh.X[b0 + g + m * ldp] : 0.0;
+          const double a1 = (g + 8 < nb && mk) ? sh.X[b0 + g + 8 + m * ldp] : 0.0;
+          const double b0v = (tn * 8 + g < nb && mk) ? sh.Y[m * ldp + b0 + tn * 8 + g] : 0.0;
+          dmma_16x8x4(acc, a0, a1, b0v);
+        }
+      }
+      if (v00) G[b0 + g + (size_t)(b0 + c) * ld] = acc[0];
+      if (v01) G[b0 + g + (size_t)(b0 + c + 1) * ld] = acc[1];
+      if (v10) G[b0 + g + 8 + (size_t)(b0 + c) * ld] = acc[2];
+      if (v11) G[b0 + g + 8 + (size_t)(b0 + c + 1) * ld] = acc[3];
+    }
+  }
+  __syncwarp();
+}
+
+template <int NB>
+__device__ void metropolis_slice_blk(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
+                                     double& n_acc, int flags, long long log_base) {
+  const int N = ch.N;
   const int ldp = panel_ld(N);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, nwarps = blockDim.x >> 5;
   const bool log = (flags & HQ_F_LOG_RATIOS) && ch.ratios;
   // uniforms of this slice: site i consumes engine draws 2i+1, 2i+2 after the current state
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+  for (int i = tid; i < N; i += blockDim.x) {
     const uint32_t x1 = minstd_mulmod(minstd_pow(2ull * i + 1), rng);
     const uint32_t x2 = minstd_mulmod(kMinstdA, x1);
     sh.u[i] = canonical_from_pair(x1, x2);
-    sh.d[i] = G[i + (size_t)i * ld];
+    sh.dl[i] = sh.s[i] > 0 ? ch.delta_p : ch.delta_m;
     sh.flip[i] = 0;
   }
   rng = minstd_mulmod(minstd_pow(2ull * N), rng);
   __syncthreads();
-  int k = 0, start = 0;
-  const int tid = threadIdx.x;
-  constexpr int kTeam = 128;  // warps 0-3 walk the decision chain, warps 4-7 fill panels
-  while (true) {
-    // The decision team walks the chain of flips of this panel. For each accepted site j it
-    // computes the entries p > j of G's current column / row j (all that later decisions of
-    // this slice read) and the diagonal; the helper warps fill the entries p <= j of the
-    // same panel columns from a shared-memory queue, off the critical path.
-    if (tid == 0) { *sh.qn = 0; *sh.qdone = 0; }
+  double acc_count = 0.0;
+  if (warp == 0) walk_block<NB>(ch, G, ld, sh, 0, min(NB, N), log, 0, acc_count);
+  for (int b0 = 0, bi = 0; b0 < N; b0 += NB, ++bi) {
+    // records and factors of block bi are complete; so is the flush of block bi-1
     __syncthreads();
-    if (tid < kTeam) {
-      int kk = 0, round = 0;
-      while (start < N && kk < kmax) {
-        // first accepted site >= start: 128 sites per round. accept iff u < min(1, |r|),
-        // r = a^2 / (1 + Delta), 1 + Delta = e^{-2 alpha s} > 0: u (1 + Delta) < a^2.
-        // gamma = Delta / a is formed speculatively by every accepting thread.
-        int j = -1;
-        for (int base = start; base < N; base += kTeam) {
-          const int i = base + tid;
-          bool acc = false;
-          if (i < N) {
-            const double delta = sh.s[i] > 0 ? ch.delta_p : ch.delta_m;
-            const double a = 1.0 + (1.0 - sh.d[i]) * delta;
-            if (log) sh.rr[i] = (a * a) / (1.0 + delta);
-            acc = sh.u[i] * (1.0 + delta) < a * a;
-            if (acc) sh.gam[tid] = delta / a;
-          }
-          const unsigned bal = __ballot_sync(0xffffffffu, acc);
-          int* wb = sh.ired + 8 + (round & 1) * 4;
-          if ((tid & 31) == 0) wb[tid >> 5] = bal ? (tid & ~31) + __ffs(bal) - 1 : kTeam;
-          team_sync();
-          ++round;
-          int first = kTeam;
-#pragma unroll
-          for (int w = 0; w < 4; ++w) first = min(first, wb[w]);
-          if (first < kTeam) { j = base + first; break; }
-        }
-        if (j < 0) { start = N; break; }
-        const double gamma = sh.gam[(j - start) % kTeam];  // written by the accepting thread of the round
-        for (int p = j + 1 + tid; p < N; p += kTeam) {
-          double c0 = G[p + (size_t)j * ld], c1 = 0.0, r0 = G[j + (size_t)p * ld], r1 = 0.0;
-          int m = 0;
-          for (; m + 1 < kk; m += 2) {
-            c0 = fma(sh.X[p + m * ldp], sh.Y[m * ldp + j], c0);
-            r0 = fma(sh.X[j + m * ldp], sh.Y[m * ldp + p], r0);
-            c1 = fma(sh.X[p + (m + 1) * ldp], sh.Y[(m + 1) * ldp + j], c1);
-            r1 = fma(sh.X[j + (m + 1) * ldp], sh.Y[(m + 1) * ldp + p], r1);
-          }
-          if (m < kk) {
-            c0 = fma(sh.X[p + m * ldp], sh.Y[m * ldp + j], c0);
-            r0 = fma(sh.X[j + m * ldp], sh.Y[m * ldp + p], r0);
-          }
-          const double xv = gamma * (c0 + c1);
-          const double yv = r0 + r1;
-          sh.X[p + kk * ldp] = xv;
-          sh.Y[kk * ldp + p] = yv;
-          sh.d[p] = fma(xv, yv, sh.d[p]);
-        }
-        if (tid == 0) {
-          sh.flip[j] = 1;
-          sh.qj[kk] = j;
-          sh.qg[kk] = gamma;
-        }
-        __threadfence_block();
-        team_sync();
-        if (tid == 0) *sh.qn = kk + 1;  // entries p > j of column kk are visible to everyone
-        n_acc += (tid == 0) ? 1.0 : 0.0;
-        ++kk;
-        start = j + 1;
+    const int a = sh.ired[bi & 1];
+    const int b0n = b0 + NB;
+    const bool next = b0n < N;
+    const int nbn = next ? min(NB, N - b0n) : 0;
+    if (a > 0) {
+      form_panels(G, ld, N, sh, ldp, a);
+      __syncthreads();
+      if (next && warp == 0) {
+        correct_block(G, ld, sh, ldp, b0n, nbn, a);
+        walk_block<NB>(ch, G, ld, sh, b0n, nbn, log, (bi + 1) & 1, acc_count);
+      } else {
+        const int w0 = next ? 1 : 0;
+        rank_update_ex(G, ld, N, N, sh.X, ldp, sh.Y, ldp, a, w0, nwarps - w0, next ? b0n : 0,
+                       next ? b0n + nbn : 0);
       }
-      if (tid == 0) {
-        sh.ired[0] = kk;
-        sh.ired[1] = start;
-        __threadfence_block();
-        *sh.qdone = 1;
-      }
-    } else {
-      // helpers: rows p <= j of every published panel column, in publication order
-      const int hid = tid - kTeam, nh = blockDim.x - kTeam;
-      int next = 0;
-      long long spins = 0;
-      while (true) {
-        int avail = *sh.qn;
-        if (next >= avail) {
-          if (*sh.qdone) {
-            __threadfence_block();
-            avail = *sh.qn;
-            if (next >= avail) break;
-          } else {
-            if (++spins > (1ll << 24)) { ch.acc[HQ_ACC_STATUS] = 2.0; break; }  // bounded wait
-            __nanosleep(64);
-            continue;
-          }
-        }
-        __threadfence_block();
-        const int j = sh.qj[next];
-        const double gamma = sh.qg[next];
-        for (int p = hid; p <= j; p += nh) {
-          double c0 = G[p + (size_t)j * ld], c1 = 0.0, r0 = G[j + (size_t)p * ld], r1 = 0.0;
-          int m = 0;
-          for (; m + 1 < next; m += 2) {
-            c0 = fma(sh.X[p + m * ldp], sh.Y[m * ldp + j], c0);
-            r0 = fma(sh.X[j + m * ldp], sh.Y[m * ldp + p], r0);
-            c1 = fma(sh.X[p + (m + 1) * ldp], sh.Y[(m + 1) * ldp + j], c1);
-            r1 = fma(sh.X[j + (m + 1) * ldp], sh.Y[(m + 1) * ldp + p], r1);
-          }
-          if (m < next) {
-            c0 = fma(sh.X[p + m * ldp], sh.Y[m * ldp + j], c0);
-            r0 = fma(sh.X[j + m * ldp], sh.Y[m * ldp + p], r0);
-          }
-          sh.X[p + next * ldp] = gamma * (c0 + c1);
-          sh.Y[next * ldp + p] = (r0 + r1) - (p == j ? 1.0 : 0.0);
-        }
-        ++next;
-      }
+    } else if (next && warp == 0) {
+      walk_block<NB>(ch, G, ld, sh, b0n, nbn, log, (bi + 1) & 1, acc_count);
     }
-    __syncthreads();
-    k = sh.ired[0];
-    start = sh.ired[1];
-    if (k > 0 && (k == kmax || start >= N)) {
-      flush_panels(G, ld, N, sh.X, ldp, sh.Y, ldp, k);
-      k = 0;
-    }
-    __syncthreads();
-    if (start >= N) break;
   }
+  __syncthreads();
+  n_acc += acc_count;
   // apply the flips of this slice and optionally log the visit-time ratios
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+  for (int i = tid; i < N; i += blockDim.x) {
     if (sh.flip[i]) sh.s[i] = -sh.s[i];
     if (log && log_base + i < ch.ratio_cap) ch.ratios[log_base + i] = sh.rr[i];
   }
   __syncthreads();
 }
 
-// ---------------------------------------------------------------------------------
-//  Register-panel Metropolis sweep of one slice (N <= blockDim.x, one site per thread).
-//
-//  Thread p owns site p: its uniform, field, current diagonal G_pp and its row of the
-//  delayed-update panels (X[p, :], Y[:, p]) live in registers. Sites of a slice are
-//  accepted in increasing order j_0 < j_1 < ..., so for a new flip j only the entries
-//  p > j of G's current column / row j can influence later decisions of the slice:
-//      col_p = G0[p, j] + sum_m X[p, m] Y[m, j],  row_p = G0[j, p] + sum_m X[j, m] Y[m, p]
-//  with Y[m, j] and X[j, m] (j > j_m) published by thread j in shared memory. The entries
-//  p <= j_m are filled just before the panel is flushed into G0 with DMMA.
-// ---------------------------------------------------------------------------------
-template <int KMAX>
-__device__ void metropolis_slice_reg(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
-                                     double& n_acc, int flags, long long log_base) {
-  const int N = ch.N;
-  const int kmax = ch.kmax < KMAX ? ch.kmax : KMAX;
-  const int ldp = panel_ld(N);
-  const int p = threadIdx.x;
-  const int lane = p & 31, warp = p >> 5, nwarps = blockDim.x >> 5;
-  const bool owner = p < N;
-  const bool log = (flags & HQ_F_LOG_RATIOS) && ch.ratios;
-  double u = 0.0, d = 0.0, dlt = 0.0, rr = 0.0;
-  bool flipped = false;
-  if (owner) {
-    const uint32_t x1 = minstd_mulmod(minstd_pow(2ull * p + 1), rng);
-    const uint32_t x2 = minstd_mulmod(kMinstdA, x1);
-    u = canonical_from_pair(x1, x2);
-    d = G[p + (size_t)p * ld];
-    dlt = sh.s[p] > 0 ? ch.delta_p : ch.delta_m;
-  }
-  rng = minstd_mulmod(minstd_pow(2ull * N), rng);
-  double Xr[KMAX], Yr[KMAX];
-#pragma unroll
-  for (int m = 0; m < KMAX; ++m) { Xr[m] = 0.0; Yr[m] = 0.0; }
-  int k = 0, start = 0, parity = 0;
-  while (true) {
-    // ---- first accepted site >= start: accept iff u (1 + Delta) < a^2 (u < min(1, |r|)) ----
-    int cand = INT_MAX;
-    if (owner && p >= start) {
-      const double a = 1.0 + (1.0 - d) * dlt;
-      if (log) rr = (a * a) / (1.0 + dlt);
-      if (u * (1.0 + dlt) < a * a) {
-        cand = p;
-        sh.gam[p] = dlt / a;  // gamma of this site, used only if it is the first
-      }
-    }
-    cand = __reduce_min_sync(0xffffffffu, cand);
-    int* wb = sh.ired + 8 + parity * 16;
-    parity ^= 1;
-    if (lane == 0) wb[warp] = cand;
-    __syncthreads();
-    int j = INT_MAX;
-    for (int w = 0; w < nwarps; ++w) j = min(j, wb[w]);
-    if (j == INT_MAX) break;
-    const double gamma = sh.gam[j];
-    // ---- append column k: entries p > j (later decisions read only those) ----
-    if (owner && p > j) {
-      double c0 = G[p + (size_t)j * ld], c1 = 0.0, r0 = G[j + (size_t)p * ld], r1 = 0.0;
-#pragma unroll
-      for (int m = 0; m < KMAX; m += 2) {
-        if (m < k) {
-          c0 = fma(Xr[m], sh.Y[m * ldp + j], c0);
-          r0 = fma(sh.X[j + m * ldp], Yr[m], r0);
-        }
-        if (m + 1 < k) {
-          c1 = fma(Xr[m + 1], sh.Y[(m + 1) * ldp + j], c1);
-          r1 = fma(sh.X[j + (m + 1) * ldp], Yr[m + 1], r1);
-        }
-      }
-      const double xv = gamma * (c0 + c1), yv = r0 + r1;
-#pragma unroll
-      for (int m = 0; m < KMAX; ++m)
-        if (m == k) { Xr[m] = xv; Yr[m] = yv; }
-      sh.X[p + k * ldp] = xv;
-      sh.Y[k * ldp + p] = yv;
-      d = fma(xv, yv, d);
-    }
-    if (p == j) flipped = true;
-    if (p == 0) { sh.qj[k] = j; sh.qg[k] = gamma; }
-    n_acc += (p == 0) ? 1.0 : 0.0;
-    ++k;
-    start = j + 1;
-    __syncthreads();
-    if (k == kmax || start >= N) {
-      // ---- fill the entries p <= j_m of the panel, then flush G0 += X Y ----
-      if (owner) {
-#pragma unroll
-        for (int m = 0; m < KMAX; ++m) {
-          if (m < k) {
-            const int jm = sh.qj[m];
-            if (p <= jm) {
-              double c = G[p + (size_t)jm * ld], r = G[jm + (size_t)p * ld];
-#pragma unroll
-              for (int m2 = 0; m2 < KMAX; ++m2)
-                if (m2 < m) {
-                  c = fma(Xr[m2], sh.Y[m2 * ldp + jm], c);
-                  r = fma(sh.X[jm + m2 * ldp], Yr[m2], r);
-                }
-              Xr[m] = sh.qg[m] * c;
-              Yr[m] = r - (p == jm ? 1.0 : 0.0);
-              sh.X[p + m * ldp] = Xr[m];
-              sh.Y[m * ldp + p] = Yr[m];
-            }
-          }
-        }
-      }
-      __syncthreads();
-      flush_panels(G, ld, N, sh.X, ldp, sh.Y, ldp, k);
-      k = 0;
-      __syncthreads();
-      if (owner) d = G[p + (size_t)p * ld];
-      if (start >= N) break;
-    }
-  }
-  if (k > 0) {
-    // a slice that ended on a round without acceptance: fill and flush the open panel
-    if (owner) {
-#pragma unroll
-      for (int m = 0; m < KMAX; ++m) {
-        if (m < k) {
-          const int jm = sh.qj[m];
-          if (p <= jm) {
-            double c = G[p + (size_t)jm * ld], r = G[jm + (size_t)p * ld];
-#pragma unroll
-            for (int m2 = 0; m2 < KMAX; ++m2)
-              if (m2 < m) {
-                c = fma(Xr[m2], sh.Y[m2 * ldp + jm], c);
-                r = fma(sh.X[jm + m2 * ldp], Yr[m2], r);
-              }
-            Xr[m] = sh.qg[m] * c;
-            Yr[m] = r - (p == jm ? 1.0 : 0.0);
-            sh.X[p + m * ldp] = Xr[m];
-            sh.Y[m * ldp + p] = Yr[m];
-          }
-        }
-      }
-    }
-    __syncthreads();
-    flush_panels(G, ld, N, sh.X, ldp, sh.Y, ldp, k);
-    __syncthreads();
-  }
-  if (owner) {
-    if (flipped) sh.s[p] = -sh.s[p];
-    if (log && log_base + p < ch.ratio_cap) ch.ratios[log_base + p] = rr;
-  }
-  __syncthreads();
-}
-
-// picks the register-panel sweep when every site has its own thread
+// block size NB of the submatrix updates: the chain's delay depth (4, 8 or 16)
 __device__ void metropolis_dispatch(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
                                     double& n_acc, int flags, long long log_base) {
-  if (ch.N <= (int)blockDim.x) {
-    if (ch.kmax <= 8) metropolis_slice_reg<8>(ch, G, ld, sh, rng, n_acc, flags, log_base);
-    else metropolis_slice_reg<16>(ch, G, ld, sh, rng, n_acc, flags, log_base);
-  } else {
-    metropolis_slice(ch, G, ld, sh, rng, n_acc, flags, log_base);
-  }
+  if (ch.kmax >= 16) metropolis_slice_blk<16>(ch, G, ld, sh, rng, n_acc, flags, log_base);
+  else if (ch.kmax >= 8) metropolis_slice_blk<8>(ch, G, ld, sh, rng, n_acc, flags, log_base);
+  else metropolis_slice_blk<4>(ch, G, ld, sh, rng, n_acc, flags, log_base);
 }
 
 // ---------------------------------------------------------------------------------
@@ -519,7 +491,7 @@ k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int 
   int ld;
   if (resident) {
     G = p;
-    ld = smem_ld(N);
+    ld = interval_ld(N);
     p += (size_t)N * ld;
     copy_mat(G, ld, ch.G, N, N);
   } else {
@@ -533,21 +505,21 @@ k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int 
   MetroShared sh;
   sh.X = work;
   sh.Y = work + (size_t)panel_ld(N) * ch.kmax;
-  sh.d = p; p += N;
+  sh.dl = p; p += N;
   sh.u = p; p += N;
   sh.rr = p; p += N;
   sh.s = reinterpret_cast<int8_t*>(p);
   sh.flip = sh.s + N;
   sh.ired = ired;
-  __shared__ int qj_s[64];
-  __shared__ double qg_s[64];
-  __shared__ double gam_s[HQ_INT_THREADS];
-  sh.gam = gam_s;
-  __shared__ int qn_s, qdone_s;
+  __shared__ int qj_s[16];
+  __shared__ double qg_s[16];
+  __shared__ double xl_s[16 * 16], yl_s[16 * 16], am_s[16 * 16], bm_s[16 * 16];
   sh.qj = qj_s;
   sh.qg = qg_s;
-  sh.qn = &qn_s;
-  sh.qdone = &qdone_s;
+  sh.xl = xl_s;
+  sh.yl = yl_s;
+  sh.Am = am_s;
+  sh.Bm = bm_s;
   uint32_t rng = *ch.rng;
   double n_acc = 0.0, n_prop = 0.0;
   long long log_base = (flags & HQ_F_LOG_RATIOS) && ch.ratio_count ? *ch.ratio_count : 0;
@@ -1019,8 +991,6 @@ __device__ __forceinline__ double vscale(const double* v, int mode, int i) {
   return fmin(x, 1.0);
 }
 
-constexpr int GBM = 64, GBN = 64, GBK = 16, GLD = 68;
-
 // 8-byte asynchronous global -> shared copy; zero-fills (reads 0 bytes of `src`, which
 // the callers keep pointing at the operand's base) when `valid` is false
 __device__ __forceinline__ void cp_async_8(double* dst, const double* src, bool valid) {
@@ -1032,57 +1002,90 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int NPEND>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND)); }
 
-__device__ __forceinline__ void gemm_load_chunk(const HqGemmJob& J, int m0, int n0, int k0, double* sA, double* sB) {
-  // op(A) tile rows m0..m0+63, cols k0..k0+15 -> sA[k][m]; op(B) rows k0..k0+15, cols n0..n0+63 -> sB[k][n]
-  for (int idx = threadIdx.x; idx < GBM * GBK; idx += blockDim.x) {
-    int m, k;
-    if (!J.ta) { m = idx % GBM; k = idx / GBM; } else { k = idx % GBK; m = idx / GBK; }
-    const int gm = m0 + m, gk = k0 + k;
-    const bool ok = gm < J.M && gk < J.K;
-    const double* src = ok ? (!J.ta ? J.A + gm + (size_t)gk * J.lda : J.A + gk + (size_t)gm * J.lda) : J.A;
-    cp_async_8(sA + k * GLD + m, src, ok);
-  }
-  for (int idx = threadIdx.x; idx < GBK * GBN; idx += blockDim.x) {
-    int k, n;
-    if (!J.tb) { k = idx % GBK; n = idx / GBK; } else { n = idx % GBN; k = idx / GBN; }
-    const int gk = k0 + k, gn = n0 + n;
-    const bool ok = gk < J.K && gn < J.Nc;
-    const double* src = ok ? (!J.tb ? J.B + gk + (size_t)gn * J.ldb : J.B + gn + (size_t)gk * J.ldb) : J.B;
-    cp_async_8(sB + k * GLD + n, src, ok);
+// ---------------------------------------------------------------------------------
+//  k_gemm: batched C = alpha op(A) diag(ks) op(B) (row / column scalings, beta, wrap-error
+//  epilogue), one CTA per 48 x 48 tile of one job (144 = 3 x 48: no padding for the 12 x 12
+//  lattice). Six warps own 16 x 24 blocks (3 DMMA tiles each); K streams through shared
+//  memory in chunks of 16 with cp.async double buffering. Shared layouts keep the fragment
+//  loads free of bank conflicts for either transpose:
+//    op(A) = A   : sA[k * kGLdm + m]     op(A) = A^T : sA[m * kGLdk + k]
+//    op(B) = B   : sB[n * kGLdk + k]     op(B) = B^T : sB[k * kGLdm + n]
+// ---------------------------------------------------------------------------------
+constexpr int kGT = 48, kGKc = 16, kGLdm = 52, kGLdk = 20, kGWarps = 6;
+constexpr int kGStage = (kGLdm * kGKc > kGT * kGLdk) ? kGLdm * kGKc : kGT * kGLdk;  // doubles
+
+// copies 2 doubles (16 B) with zero fill of the invalid part; both addresses 16-byte aligned
+__device__ __forceinline__ void cp_async_16(double* dst, const double* src, int nvalid) {
+  const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  const int nbytes = nvalid <= 0 ? 0 : (nvalid >= 2 ? 16 : 8);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(src), "r"(nbytes));
+}
+
+// stages the chunk [k0, k0 + 16) x [r0, r0 + 48) of op(X) (r = m for A, n for B; R rows).
+// kmaj: op(X) is contiguous along k in memory (A^T or B) -> layout [r][k]; otherwise
+// contiguous along r -> layout [k][r]. `pair` selects 16-byte copies (even ld, aligned base).
+__device__ __forceinline__ void g_stage(const double* X, int ldx, bool kmaj, int R, int K, int r0, int k0,
+                                        double* sX, bool pair) {
+  if (pair) {
+    if (kmaj) {
+      for (int idx = threadIdx.x; idx < kGT * (kGKc / 2); idx += blockDim.x) {
+        const int r = idx / (kGKc / 2), k = 2 * (idx % (kGKc / 2));
+        const int nv = (r0 + r < R) ? min(2, K - (k0 + k)) : 0;
+        cp_async_16(sX + r * kGLdk + k, nv > 0 ? X + (k0 + k) + (size_t)(r0 + r) * ldx : X, nv);
+      }
+    } else {
+      for (int idx = threadIdx.x; idx < (kGT / 2) * kGKc; idx += blockDim.x) {
+        const int r = 2 * (idx % (kGT / 2)), k = idx / (kGT / 2);
+        const int nv = (k0 + k < K) ? min(2, R - (r0 + r)) : 0;
+        cp_async_16(sX + k * kGLdm + r, nv > 0 ? X + (r0 + r) + (size_t)(k0 + k) * ldx : X, nv);
+      }
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < kGT * kGKc; idx += blockDim.x) {
+      int r, k;
+      if (kmaj) { r = idx / kGKc; k = idx % kGKc; } else { r = idx % kGT; k = idx / kGT; }
+      const bool ok = k0 + k < K && r0 + r < R;
+      const double* src = ok ? (kmaj ? X + (k0 + k) + (size_t)(r0 + r) * ldx : X + (r0 + r) + (size_t)(k0 + k) * ldx) : X;
+      cp_async_8(kmaj ? sX + r * kGLdk + k : sX + k * kGLdm + r, src, ok);
+    }
   }
 }
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kGWarps * 32, 4)
 k_gemm(const HqGemmJob* __restrict__ jobs, int njobs, int tiles_n) {
-  __shared__ __align__(16) double sA[2][GBK * GLD];
-  __shared__ __align__(16) double sB[2][GBK * GLD];
-  __shared__ double sK[2][GBK];
+  __shared__ __align__(16) double sA[2][kGStage];
+  __shared__ __align__(16) double sB[2][kGStage];
+  __shared__ double sK[2][kGKc];
   __shared__ double red[32];
   const int jb = blockIdx.y;
   if (jb >= njobs) return;
   const HqGemmJob J = jobs[jb];
   if (!J.active) return;
-  const int tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
-  const int m0 = tm * GBM, n0 = tn * GBN;
+  const int m0 = (blockIdx.x / tiles_n) * kGT, n0 = (blockIdx.x % tiles_n) * kGT;
   if (m0 >= J.M || n0 >= J.Nc) return;
+  const bool amaj = J.ta != 0;  // op(A) = A^T is contiguous along k
+  const bool bmaj = J.tb == 0;  // op(B) = B is contiguous along k
+  const bool pa = (J.lda % 2 == 0) && ((reinterpret_cast<uintptr_t>(J.A) & 15) == 0);
+  const bool pb = (J.ldb % 2 == 0) && ((reinterpret_cast<uintptr_t>(J.B) & 15) == 0);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, q = lane & 3;
-  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-  double acc[2][4][4];
+  const int wm = (warp % 3) * 16, wn = (warp / 3) * 24;
+  double acc[3][4];
 #pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = acc[a][b][2] = acc[a][b][3] = 0.0;
-  const int nchunks = (J.K + GBK - 1) / GBK;
-  gemm_load_chunk(J, m0, n0, 0, sA[0], sB[0]);
-  if (threadIdx.x < GBK) sK[0][threadIdx.x] = (threadIdx.x < J.K) ? vscale(J.ks, J.ks_mode, threadIdx.x) : 0.0;
+  for (int j = 0; j < 3; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+  const int nchunks = (J.K + kGKc - 1) / kGKc;
+  g_stage(J.A, J.lda, amaj, J.M, J.K, m0, 0, sA[0], pa);
+  g_stage(J.B, J.ldb, bmaj, J.Nc, J.K, n0, 0, sB[0], pb);
+  if (threadIdx.x < kGKc) sK[0][threadIdx.x] = (threadIdx.x < J.K) ? vscale(J.ks, J.ks_mode, threadIdx.x) : 0.0;
   cp_async_commit();
   for (int c = 0; c < nchunks; ++c) {
     const int cur = c & 1;
     if (c + 1 < nchunks) {
-      const int k1 = (c + 1) * GBK;
-      gemm_load_chunk(J, m0, n0, k1, sA[cur ^ 1], sB[cur ^ 1]);
-      if (threadIdx.x < GBK) sK[cur ^ 1][threadIdx.x] = (k1 + threadIdx.x < J.K) ? vscale(J.ks, J.ks_mode, k1 + threadIdx.x) : 0.0;
+      const int k1 = (c + 1) * kGKc;
+      g_stage(J.A, J.lda, amaj, J.M, J.K, m0, k1, sA[cur ^ 1], pa);
+      g_stage(J.B, J.ldb, bmaj, J.Nc, J.K, n0, k1, sB[cur ^ 1], pb);
+      if (threadIdx.x < kGKc)
+        sK[cur ^ 1][threadIdx.x] = (k1 + threadIdx.x < J.K) ? vscale(J.ks, J.ks_mode, k1 + threadIdx.x) : 0.0;
     }
     cp_async_commit();
     cp_async_wait<1>();
@@ -1090,43 +1093,39 @@ k_gemm(const HqGemmJob* __restrict__ jobs, int njobs, int tiles_n) {
     const double* A_ = sA[cur];
     const double* B_ = sB[cur];
 #pragma unroll
-    for (int kk = 0; kk < GBK; kk += 4) {
-      double a[2][2], bb[4];
-      const double kscale = sK[cur][kk + q];
+    for (int kk = 0; kk < kGKc; kk += 4) {
+      const int k = kk + q;
+      const double ksc = sK[cur][k];
+      const int m = wm + g;
+      const double a0 = (amaj ? A_[m * kGLdk + k] : A_[k * kGLdm + m]) * ksc;
+      const double a1 = (amaj ? A_[(m + 8) * kGLdk + k] : A_[k * kGLdm + m + 8]) * ksc;
 #pragma unroll
-      for (int a_ = 0; a_ < 2; ++a_) {
-        a[a_][0] = A_[(kk + q) * GLD + wm + a_ * 16 + g] * kscale;
-        a[a_][1] = A_[(kk + q) * GLD + wm + a_ * 16 + g + 8] * kscale;
+      for (int j = 0; j < 3; ++j) {
+        const int n = wn + j * 8 + g;
+        const double b0 = bmaj ? B_[n * kGLdk + k] : B_[k * kGLdm + n];
+        dmma_16x8x4(acc[j], a0, a1, b0);
       }
-#pragma unroll
-      for (int b_ = 0; b_ < 4; ++b_) bb[b_] = B_[(kk + q) * GLD + wn + b_ * 8 + g];
-#pragma unroll
-      for (int a_ = 0; a_ < 2; ++a_)
-#pragma unroll
-        for (int b_ = 0; b_ < 4; ++b_) dmma_16x8x4(acc[a_][b_], a[a_][0], a[a_][1], bb[b_]);
     }
     __syncthreads();
   }
   cp_async_wait<0>();
-  // epilogue
+  // epilogue: alpha, row / column scalings, beta, wrap-error maximum
   double emax = -INFINITY;
 #pragma unroll
-  for (int a_ = 0; a_ < 2; ++a_)
+  for (int j = 0; j < 3; ++j)
 #pragma unroll
-    for (int b_ = 0; b_ < 4; ++b_)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int gm = m0 + wm + a_ * 16 + g + ((e & 2) ? 8 : 0);
-        const int gn = n0 + wn + b_ * 8 + 2 * q + (e & 1);
-        if (gm < J.M && gn < J.Nc) {
-          double v = J.alpha * acc[a_][b_][e] * vscale(J.rs, J.rs_mode, gm) * vscale(J.cs, J.cs_mode, gn);
-          double* cp = J.C + gm + (size_t)gn * J.ldc;
-          const double old = (J.beta != 0.0 || J.epi == 1) ? *cp : 0.0;
-          if (J.beta != 0.0) v = fma(J.beta, old, v);
-          if (J.epi == 1) emax = fmax(emax, v - old);
-          *cp = v;
-        }
+    for (int e = 0; e < 4; ++e) {
+      const int gm = m0 + wm + g + ((e & 2) ? 8 : 0);
+      const int gn = n0 + wn + j * 8 + 2 * q + (e & 1);
+      if (gm < J.M && gn < J.Nc) {
+        double v = J.alpha * acc[j][e] * vscale(J.rs, J.rs_mode, gm) * vscale(J.cs, J.cs_mode, gn);
+        double* cp = J.C + gm + (size_t)gn * J.ldc;
+        const double old = (J.beta != 0.0 || J.epi == 1) ? *cp : 0.0;
+        if (J.beta != 0.0) v = fma(J.beta, old, v);
+        if (J.epi == 1) emax = fmax(emax, v - old);
+        *cp = v;
       }
+    }
   if (J.epi == 1 && J.err_out) {
     emax = block_max(emax, red);
     if (threadIdx.x == 0) atomic_max_double(J.err_out, emax);
@@ -1452,6 +1451,18 @@ static cudaError_t raise_smem(int slot, const void* fn, size_t bytes) {
 
 // sets the dynamic shared-memory limits of every per-chain kernel (outside any stream
 // capture) so that chains of up to Nmax sites can be launched
+size_t max_static_smem() {
+  const void* fns[] = {(const void*)k_interval, (const void*)k_bchain, (const void*)k_udt,
+                       (const void*)k_invert, (const void*)k_dyn_slices, (const void*)k_adj_interval};
+  size_t m = 0;
+  for (const void* f : fns) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, f) != cudaSuccess) return 16384;  // conservative
+    m = a.sharedSizeBytes > m ? a.sharedSizeBytes : m;
+  }
+  return m;
+}
+
 cudaError_t prepare_kernels(int Nmax, int kmax, bool resident) {
   const size_t mat_stage = smem_matrix_bytes(Nmax, resident, 8 * (((Nmax + 15) & ~15) + 4) + 64);
   cudaError_t e;
@@ -1487,9 +1498,9 @@ cudaError_t launch_invert(const HqChain* chains, int n, int b, int which, int Nm
 }
 cudaError_t launch_gemm(const HqGemmJob* jobs, int njobs, int Mmax, int Nmax, cudaStream_t st) {
   if (njobs <= 0) return cudaSuccess;
-  const int tm = (Mmax + GBM - 1) / GBM, tn = (Nmax + GBN - 1) / GBN;
+  const int tm = (Mmax + kGT - 1) / kGT, tn = (Nmax + kGT - 1) / kGT;
   dim3 grid(tm * tn, njobs);
-  k_gemm<<<grid, 128, 0, st>>>(jobs, njobs, tn);
+  k_gemm<<<grid, kGWarps * 32, 0, st>>>(jobs, njobs, tn);
   return cudaGetLastError();
 }
 cudaError_t launch_measure(const HqChain* chains, int n, int dir, int b, int flags, cudaStream_t st) {

@@ -9,6 +9,8 @@ size_t smem_interval_bytes(int Nmax, int kmax, bool resident);
 size_t smem_matrix_bytes(int Nmax, bool resident, int extra_doubles);
 size_t smem_invert_bytes(int Nmax, bool resident);
 size_t smem_udt_bytes(int Nmax, bool resident);
+// largest static shared memory of the kernels that take dynamic shared memory
+size_t max_static_smem();
 cudaError_t prepare_kernels(int Nmax, int kmax, bool resident);
 cudaError_t launch_interval(const HqChain* chains, int n, int dir, int b, int flags, int Nmax, int kmax, bool resident,
                             cudaStream_t st);

@@ -71,7 +71,7 @@ typedef struct hq_chain_params {
   int stabilization_pace; /* [MonteCarlo] stabilization_pace */
   int expk_mode;          /* HQ_EXPK_* ([MonteCarlo] is_fft maps to HQ_EXPK_SEPARABLE) */
   long long seed;         /* Utils::Random::set_seed(seed) before set_ising_fields_to_random */
-  int delay_depth;        /* rank-k delay depth; 0 = largest that fits on chip */
+  int delay_depth;        /* sites per submatrix-update block (4, 8 or 16; others round down, min 4); 0 = largest that fits on chip */
   int dynamic;            /* 1: allocate the displaced G's (time-displaced measurements) */
   int snapshots;          /* 1: allocate per-slice G(tau,tau) storage (HQ_SWEEP_SNAPSHOT) */
 } hq_chain_params;
