@@ -129,9 +129,12 @@ __device__ inline void atomic_max_double(double* addr, double val) {
 //  side 0: M <- c (A(x)A) M  (rows);  side 1: M <- c M (A(x)A)  (columns).
 //  rows/cols outside [0, N) are untouched. All threads of the block participate.
 // ------------------------------------------------------------------------------------
-template <int L>
+// SC selects an optional diagonal scaling fused into the pass: element (i, j) is multiplied by
+// (s[i] > 0 ? rp : rm) * (s[j] > 0 ? cp : cm), on load (SC = 1, before the convolution) or
+// on store (SC = 2); SC = 0 leaves the pass unscaled
+template <int L, int SC>
 __device__ inline void sep_pass(double* M, int ld, int N, const double* __restrict__ coef, double c, int side,
-                                int pass) {
+                                int pass, const int8_t* sf, double rp, double rm, double cp, double cm) {
   // circulant coefficients in registers (compile-time indices after unrolling)
   double a[L];
 #pragma unroll
@@ -145,9 +148,24 @@ __device__ inline void sep_pass(double* M, int ld, int N, const double* __restri
     const int step_site = (pass == 0) ? 1 : L;
     double* base = (side == 0) ? (M + base_site + (size_t)line * ld) : (M + line + (size_t)base_site * ld);
     const size_t stride = (side == 0) ? (size_t)step_site : (size_t)step_site * ld;
+    // the factor of element e is (row factor) * (column factor); side 0: the line is column
+    // j and the site row i; side 1: the line is row i and the site column j
+    double lf = 1.0, sp = 1.0, sm = 1.0;
+    if (SC) {
+      const bool lpos = sf[line] > 0;
+      lf = (side == 0) ? (lpos ? cp : cm) : (lpos ? rp : rm);
+      sp = (side == 0) ? rp : cp;
+      sm = (side == 0) ? rm : cm;
+    }
     double v[L];
 #pragma unroll
-    for (int e = 0; e < L; ++e) v[e] = base[e * stride];
+    for (int e = 0; e < L; ++e) {
+      v[e] = base[e * stride];
+      if (SC == 1) {
+        const double sfac = sf[base_site + e * step_site] > 0 ? sp : sm;
+        v[e] *= (side == 0) ? sfac * lf : lf * sfac;
+      }
+    }
     // L independent accumulators, each summed over e2 in ascending order
     double acc[L];
 #pragma unroll
@@ -158,37 +176,41 @@ __device__ inline void sep_pass(double* M, int ld, int N, const double* __restri
       for (int e = 0; e < L; ++e) acc[e] = fma(a[(e - e2 + L) % L], v[e2], acc[e]);
     }
 #pragma unroll
-    for (int e = 0; e < L; ++e) base[e * stride] = (pass == 1) ? acc[e] * c : acc[e];
+    for (int e = 0; e < L; ++e) {
+      double out = (pass == 1) ? acc[e] * c : acc[e];
+      if (SC == 2) {
+        const double sfac = sf[base_site + e * step_site] > 0 ? sp : sm;
+        out *= (side == 0) ? sfac * lf : lf * sfac;
+      }
+      base[e * stride] = out;
+    }
   }
 }
 
-template <int L>
-__device__ inline void sep_apply(double* M, int ld, int N, const double* a, double c, int side) {
-  sep_pass<L>(M, ld, N, a, c, side, 0);
+// both passes of one side; SC0 / SC1 select the fused scaling of pass 0 / pass 1
+template <int L, int SC0 = 0, int SC1 = 0>
+__device__ inline void sep_apply(double* M, int ld, int N, const double* a, double c, int side,
+                                 const int8_t* sf = nullptr, double rp = 1.0, double rm = 1.0, double cp = 1.0,
+                                 double cm = 1.0) {
+  sep_pass<L, SC0>(M, ld, N, a, c, side, 0, sf, rp, rm, cp, cm);
   __syncthreads();
-  sep_pass<L>(M, ld, N, a, c, side, 1);
+  sep_pass<L, SC1>(M, ld, N, a, c, side, 1, sf, rp, rm, cp, cm);
   __syncthreads();
 }
 
 // dispatch on the lattice size to an exact compile-time fiber length (L <= HQ_MAX_L)
-__device__ inline void sep_apply_any(double* M, int ld, int N, int L, const double* a, double c, int side) {
+template <int SC0 = 0, int SC1 = 0>
+__device__ inline void sep_apply_any(double* M, int ld, int N, int L, const double* a, double c, int side,
+                                     const int8_t* sf = nullptr, double rp = 1.0, double rm = 1.0,
+                                     double cp = 1.0, double cm = 1.0) {
   switch (L) {
-    case 1: sep_apply<1>(M, ld, N, a, c, side); break;
-    case 2: sep_apply<2>(M, ld, N, a, c, side); break;
-    case 3: sep_apply<3>(M, ld, N, a, c, side); break;
-    case 4: sep_apply<4>(M, ld, N, a, c, side); break;
-    case 5: sep_apply<5>(M, ld, N, a, c, side); break;
-    case 6: sep_apply<6>(M, ld, N, a, c, side); break;
-    case 7: sep_apply<7>(M, ld, N, a, c, side); break;
-    case 8: sep_apply<8>(M, ld, N, a, c, side); break;
-    case 9: sep_apply<9>(M, ld, N, a, c, side); break;
-    case 10: sep_apply<10>(M, ld, N, a, c, side); break;
-    case 11: sep_apply<11>(M, ld, N, a, c, side); break;
-    case 12: sep_apply<12>(M, ld, N, a, c, side); break;
-    case 13: sep_apply<13>(M, ld, N, a, c, side); break;
-    case 14: sep_apply<14>(M, ld, N, a, c, side); break;
-    case 15: sep_apply<15>(M, ld, N, a, c, side); break;
-    default: sep_apply<16>(M, ld, N, a, c, side); break;
+#define HQ_SEP_CASE(n) \
+  case n: sep_apply<n, SC0, SC1>(M, ld, N, a, c, side, sf, rp, rm, cp, cm); break;
+    HQ_SEP_CASE(1) HQ_SEP_CASE(2) HQ_SEP_CASE(3) HQ_SEP_CASE(4) HQ_SEP_CASE(5) HQ_SEP_CASE(6)
+    HQ_SEP_CASE(7) HQ_SEP_CASE(8) HQ_SEP_CASE(9) HQ_SEP_CASE(10) HQ_SEP_CASE(11) HQ_SEP_CASE(12)
+    HQ_SEP_CASE(13) HQ_SEP_CASE(14) HQ_SEP_CASE(15)
+#undef HQ_SEP_CASE
+    default: sep_apply<16, SC0, SC1>(M, ld, N, a, c, side, sf, rp, rm, cp, cm); break;
   }
 }
 

@@ -91,23 +91,20 @@ __device__ void copy_mat(double* dst, int ldd, const double* src, int lds, int N
 //      decision of the block reads only g's diagonal). For the a accepted flips
 //      j_0 < j_1 < ... it records gamma_m, X[J, m] = gamma_m g[:, j_m] and
 //      Y[m, J] = g[j_m, :] - e_{j_m}^T (g before flip m);
-//   2. the sequential updates compose to G_new = G + X Y with
-//        X = G[:, Ja] Gamma (I - C Gamma)^-1,   C[m', m] = Y[m', j_m]  (strictly upper)
-//        Y = (I - D)^-1 (G[Ja, :] - E),         D[m, m'] = X[j_m, m']  (strictly lower)
-//      the walking warp forms the two a x a unit-triangular inverses from its records,
-//      and X, Y are two small DMMA products over all warps;
-//   3. G += X Y by DMMA (rank a <= NB). While warps 1.. flush block b, warp 0 applies
-//      the same update to the next block's diagonal tile G[J', J'] (which the flush
-//      skips) and walks block b+1.
+//   2. the a flips become the panels of G_new = G + X Y,
+//        X[:, m] = gamma_m (G[:, j_m] + sum_{m'<m} X[:, m'] Y[m', j_m])
+//        Y[m, :] = G[j_m, :] - e_{j_m}^T + sum_{m'<m} X[j_m, m'] Y[m', :]
+//      one row of X and one column of Y per thread, with the coefficients X[J, :] and
+//      Y[:, J] from the walk's records;
+//   3. G += X Y by DMMA (rank a <= NB) over all warps.
 //  The result equals the reference's sequence of rank-1 updates up to rounding.
 // ---------------------------------------------------------------------------------
 // G[0:M, 0:Nc] += X[0:M, 0:k] Y[0:k, 0:Nc]  (X column-major ldx, Y row-major ldy, k <= 16),
 // by 16 x 32 strips of four 16 x 8 DMMA tiles that share the A fragments; the fragments of
-// all k-steps are loaded before the strip's G tiles so that their latencies overlap.
-// Warps w0 .. w0+nw-1 take part; elements with both indices in [ex0, ex1) are left alone.
-__device__ void rank_update_ex(double* G, int ld, int M, int Nc, const double* X, int ldx, const double* Y,
-                               int ldy, int k, int w0, int nw, int ex0, int ex1) {
-  const int lane = threadIdx.x & 31, warp = (threadIdx.x >> 5) - w0;
+// all k-steps are loaded before the strip's G tiles so that their latencies overlap
+__device__ void rank_update(double* G, int ld, int M, int Nc, const double* X, int ldx, const double* Y, int ldy,
+                            int k) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int mt = (M + 15) / 16, ns = (Nc + 31) / 32;
   const int strips = mt * ns;
@@ -128,23 +125,14 @@ __device__ void rank_update_ex(double* G, int ld, int M, int Nc, const double* X
         fb[s][t] = (cb < Nc && mk) ? Y[m * ldy + cb] : 0.0;
       }
     }
-    // element masks: in range and outside the excluded tile
-    const bool rin0 = r < M && !(r >= ex0 && r < ex1), rin1 = r + 8 < M && !(r + 8 >= ex0 && r + 8 < ex1);
-    const bool rok0 = r < M, rok1 = r + 8 < M;
     double acc[4][4];
-    bool w[4][4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       const int c = c0 + t * 8 + 2 * q;
-      const bool cx0 = c >= ex0 && c < ex1, cx1 = c + 1 >= ex0 && c + 1 < ex1;
-      w[t][0] = rok0 && c < Nc && (rin0 || !cx0);
-      w[t][1] = rok0 && c + 1 < Nc && (rin0 || !cx1);
-      w[t][2] = rok1 && c < Nc && (rin1 || !cx0);
-      w[t][3] = rok1 && c + 1 < Nc && (rin1 || !cx1);
-      acc[t][0] = w[t][0] ? G[r + (size_t)c * ld] : 0.0;
-      acc[t][1] = w[t][1] ? G[r + (size_t)(c + 1) * ld] : 0.0;
-      acc[t][2] = w[t][2] ? G[r + 8 + (size_t)c * ld] : 0.0;
-      acc[t][3] = w[t][3] ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
+      acc[t][0] = (r < M && c < Nc) ? G[r + (size_t)c * ld] : 0.0;
+      acc[t][1] = (r < M && c + 1 < Nc) ? G[r + (size_t)(c + 1) * ld] : 0.0;
+      acc[t][2] = (r + 8 < M && c < Nc) ? G[r + 8 + (size_t)c * ld] : 0.0;
+      acc[t][3] = (r + 8 < M && c + 1 < Nc) ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
     }
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
@@ -156,17 +144,12 @@ __device__ void rank_update_ex(double* G, int ld, int M, int Nc, const double* X
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       const int c = c0 + t * 8 + 2 * q;
-      if (w[t][0]) G[r + (size_t)c * ld] = acc[t][0];
-      if (w[t][1]) G[r + (size_t)(c + 1) * ld] = acc[t][1];
-      if (w[t][2]) G[r + 8 + (size_t)c * ld] = acc[t][2];
-      if (w[t][3]) G[r + 8 + (size_t)(c + 1) * ld] = acc[t][3];
+      if (r < M && c < Nc) G[r + (size_t)c * ld] = acc[t][0];
+      if (r < M && c + 1 < Nc) G[r + (size_t)(c + 1) * ld] = acc[t][1];
+      if (r + 8 < M && c < Nc) G[r + 8 + (size_t)c * ld] = acc[t][2];
+      if (r + 8 < M && c + 1 < Nc) G[r + 8 + (size_t)(c + 1) * ld] = acc[t][3];
     }
   }
-}
-
-__device__ void rank_update(double* G, int ld, int M, int Nc, const double* X, int ldx, const double* Y, int ldy,
-                            int k) {
-  rank_update_ex(G, ld, M, Nc, X, ldx, Y, ldy, k, 0, blockDim.x >> 5, 0, 0);
 }
 
 // G += X Y on the full N x N matrix (the flush of the delayed Metropolis panels)
@@ -182,10 +165,8 @@ struct MetroShared {
   int8_t* flip;   // accepted flags [N]
   double* X;      // N x 16 panel (column-major, ld panel_ld(N))
   double* Y;      // 16 x N panel (row-major, ld panel_ld(N))
-  double* xl;     // X[J, m] of the block: xl[m * NB + s]
-  double* yl;     // Y[m, J] of the block: yl[m * NB + s]
-  double* Am;     // Gamma (I - C Gamma)^-1, 16 x 16 row-major, zero outside a x a
-  double* Bm;     // (I - D)^-1, 16 x 16 row-major, zero outside a x a
+  double* xt;     // X[J_s, m] of the block at xt[s * NB + m] (16-byte aligned)
+  double* yt;     // Y[m, J_s] of the block at yt[s * NB + m] (16-byte aligned)
   int* ired;      // >= 8 ints
   int* qj;        // accepted site of each panel column [16]
   double* qg;     // gamma of each panel column [16]
@@ -216,9 +197,15 @@ __device__ void walk_block(const HqChain& ch, const double* G, int ld, const Met
     dls[s] = s < nb ? sh.dl[b0 + s] : 0.0;
     thr[s] = s < nb ? sh.u[b0 + s] * (1.0 + dls[s]) : 0.0;
   }
-  int a = 0;
+  // per-site records stay in registers during the walk (shared-memory stores would queue
+  // with the shuffles on the same pipe): xk[s] = X[J_row, s] for the row this lane writes,
+  // yk[s] = Y[s, J_c], the acceptance mask and, in lane s, gamma_s and the visit ratio
+  double xk[NB], yk[NB], myg = 0.0, myr = 0.0;
+  unsigned mask = 0u;
 #pragma unroll
   for (int s = 0; s < NB; ++s) {
+    xk[s] = 0.0;
+    yk[s] = 0.0;
     if (s < nb) {
       const int ss = s / R, si = s % R;  // g[s][*] is held by group ss at register si
       // column s, row s and the diagonal entry of the current g; gamma is formed before
@@ -231,145 +218,144 @@ __device__ void walk_block(const HqChain& ch, const double* G, int ld, const Met
       const double dl = dls[s];
       const double av = 1.0 + (1.0 - dg) * dl;
       const double gam = dl / av;
-      if (log && lane == 0) sh.rr[b0 + s] = (av * av) / (1.0 + dl);
+      if (log && lane == s) myr = (av * av) / (1.0 + dl);
       // accept iff u < min(1, |r|), r = a^2 / (1 + Delta), 1 + Delta = e^{-2 alpha s} > 0
-      if (thr[s] < av * av) {
-        double colv[R];
+      const bool acc = thr[s] < av * av;
+      const double ge = acc ? gam : 0.0;
+      double xs = colr[0];
 #pragma unroll
-        for (int i = 0; i < R; ++i) {
-          colv[i] = gam * colr[i];
-          r[i] = fma(colv[i], yv, r[i]);
-        }
-        if (writer && c == 0) {
+      for (int i = 1; i < R; ++i) xs = (c == i) ? colr[i] : xs;
+      xk[s] = ge * xs;
+      yk[s] = yv;
+      if (lane == s) myg = gam;
 #pragma unroll
-          for (int i = 0; i < R; ++i) sh.xl[a * NB + h * R + i] = colv[i];
-        }
-        if (writer && h == 0) sh.yl[a * NB + c] = yv;
-        if (lane == 0) {
-          sh.qj[a] = b0 + s;
-          sh.qg[a] = gam;
-          sh.flip[b0 + s] = 1;
-        }
-        ++a;
-      }
+      for (int i = 0; i < R; ++i) r[i] = fma(ge * colr[i], yv, r[i]);
+      mask |= acc ? (1u << s) : 0u;
     }
+  }
+  // the records of the accepted flips, in acceptance order
+  const int a = __popc(mask);
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    if (mask & (1u << s)) {
+      const int m = __popc(mask & ((1u << s) - 1u));
+      if (writer && c < R) sh.xt[(h * R + c) * NB + m] = xk[s];
+      if (writer && h == 0) sh.yt[c * NB + m] = yk[s];
+    }
+  }
+  if (lane < nb) {
+    const bool acc = (mask >> lane) & 1u;
+    if (acc) {
+      const int m = __popc(mask & ((1u << lane) - 1u));
+      sh.qj[m] = b0 + lane;
+      sh.qg[m] = myg;
+    }
+    sh.flip[b0 + lane] = acc ? 1 : 0;
+    if (log) sh.rr[b0 + lane] = myr;
   }
   if (lane == 0) sh.ired[slot] = a;
   acc_count += (lane == 0) ? (double)a : 0.0;
-  __syncwarp();
-  // unit-triangular inverses: lanes 0-15 row r of T = (I - C Gamma)^-1 (then A = Gamma T),
-  // lanes 16-31 column r of B = (I - D)^-1; both follow V[m] = delta_rm + s_m sum_{m'<m}
-  // V[m'] coef[m'][m] with coef read from the walk's records
-  const int rr_ = lane & 15;
-  const bool aside = lane < 16;
-  const double* cf = aside ? sh.yl : sh.xl;
-  double V[16];
-#pragma unroll
-  for (int m = 0; m < 16; ++m) {
-    V[m] = 0.0;
-    if (m < a) {
-      const int sj = sh.qj[m] - b0;
-      double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-      for (int m2 = 0; m2 + 1 < m; m2 += 2) {
-        s0 = fma(V[m2], cf[m2 * NB + sj], s0);
-        s1 = fma(V[m2 + 1], cf[(m2 + 1) * NB + sj], s1);
-      }
-      if (m & 1) s0 = fma(V[m - 1], cf[(m - 1) * NB + sj], s0);
-      V[m] = (m == rr_ ? 1.0 : 0.0) + (aside ? sh.qg[m] : 1.0) * (s0 + s1);
-    }
-  }
-  const double sc = (rr_ < a) ? (aside ? sh.qg[rr_] : 1.0) : 0.0;
-#pragma unroll
-  for (int m = 0; m < 16; ++m) {
-    if (aside) sh.Am[rr_ * 16 + m] = sc * V[m];
-    else sh.Bm[m * 16 + rr_] = sc * V[m];
-  }
 }
 
-// X = G[:, Ja] A (N x 16) and Y = B (G[Ja, :] - E) (16 x N) into the panels, all warps
-__device__ void form_panels(const double* G, int ld, int N, const MetroShared& sh, int ldp, int a) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int g = lane >> 2, q = lane & 3;
-  const int mt = (N + 15) / 16, ntx = a > 8 ? 2 : 1, nty = (N + 7) / 8;
-  const int ksteps = (a + 3) >> 2;
-  int jq[4];
+// panels of the a flips of block [b0, b0 + NB): the two triangular recurrences, one row of X
+// and one column of Y per thread; the coefficients of flip m are contiguous in the records
+// (xt / yt at row j_m - b0) and are read in 16-byte pairs
+template <int NB>
+__device__ void build_panels(const double* G, int ld, int N, const MetroShared& sh, int ldp, int a, int b0) {
+  for (int p = threadIdx.x; p < N; p += blockDim.x) {
+    double x[NB], y[NB];
 #pragma unroll
-  for (int s = 0; s < 4; ++s) jq[s] = (4 * s + q < a) ? sh.qj[4 * s + q] : 0;
-  for (int ti = warp; ti < mt * ntx + nty; ti += nwarps) {
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (ti < mt * ntx) {
-      const int r = (ti % mt) * 16 + g, n0 = (ti / mt) * 8;
+    for (int m = 0; m < NB; ++m) {
+      x[m] = 0.0;
+      y[m] = 0.0;
+      if (m < a) {
+        const int jm = sh.qj[m], sj = jm - b0;
+        const double* cy = sh.yt + sj * NB;  // Y[m2, j_m]
+        const double* cx = sh.xt + sj * NB;  // X[j_m, m2]
+        double cx0 = G[p + (size_t)jm * ld], cx1 = 0.0;
+        double cy0 = G[jm + (size_t)p * ld] - (p == jm ? 1.0 : 0.0), cy1 = 0.0;
 #pragma unroll
-      for (int s = 0; s < 4; ++s) {
-        if (s < ksteps) {
-          const bool mk = 4 * s + q < a;
-          const double a0 = (r < N && mk) ? G[r + (size_t)jq[s] * ld] : 0.0;
-          const double a1 = (r + 8 < N && mk) ? G[r + 8 + (size_t)jq[s] * ld] : 0.0;
-          const double b0 = sh.Am[(4 * s + q) * 16 + n0 + g];
-          dmma_16x8x4(acc, a0, a1, b0);
+        for (int m2 = 0; m2 + 1 < m; m2 += 2) {
+          const double2 vy = *reinterpret_cast<const double2*>(cy + m2);
+          const double2 vx = *reinterpret_cast<const double2*>(cx + m2);
+          cx0 = fma(x[m2], vy.x, cx0);
+          cx1 = fma(x[m2 + 1], vy.y, cx1);
+          cy0 = fma(vx.x, y[m2], cy0);
+          cy1 = fma(vx.y, y[m2 + 1], cy1);
         }
-      }
-      // the panels hold a <= delay depth columns / rows
-      const int cc = n0 + 2 * q;
-      if (r < N && cc < a) sh.X[r + cc * ldp] = acc[0];
-      if (r < N && cc + 1 < a) sh.X[r + (cc + 1) * ldp] = acc[1];
-      if (r + 8 < N && cc < a) sh.X[r + 8 + cc * ldp] = acc[2];
-      if (r + 8 < N && cc + 1 < a) sh.X[r + 8 + (cc + 1) * ldp] = acc[3];
-    } else {
-      const int n0 = (ti - mt * ntx) * 8, n = n0 + g;
-#pragma unroll
-      for (int s = 0; s < 4; ++s) {
-        if (s < ksteps) {
-          const int m = 4 * s + q;
-          const double a0 = sh.Bm[g * 16 + m], a1 = sh.Bm[(g + 8) * 16 + m];
-          const double b0 = (n < N && m < a) ? G[jq[s] + (size_t)n * ld] - (n == jq[s] ? 1.0 : 0.0) : 0.0;
-          dmma_16x8x4(acc, a0, a1, b0);
+        if (m & 1) {
+          cx0 = fma(x[m - 1], cy[m - 1], cx0);
+          cy0 = fma(cx[m - 1], y[m - 1], cy0);
         }
+        x[m] = sh.qg[m] * (cx0 + cx1);
+        y[m] = cy0 + cy1;
       }
-      const int cc = n0 + 2 * q;
-      if (cc < N && g < a) sh.Y[g * ldp + cc] = acc[0];
-      if (cc + 1 < N && g < a) sh.Y[g * ldp + cc + 1] = acc[1];
-      if (cc < N && g + 8 < a) sh.Y[(g + 8) * ldp + cc] = acc[2];
-      if (cc + 1 < N && g + 8 < a) sh.Y[(g + 8) * ldp + cc + 1] = acc[3];
+    }
+    // stores after the recurrence: the loads above are free to run ahead of them
+#pragma unroll
+    for (int m = 0; m < NB; ++m) {
+      if (m < a) {
+        sh.X[p + m * ldp] = x[m];
+        sh.Y[m * ldp + p] = y[m];
+      }
     }
   }
 }
 
-// warp 0: G[J', J'] += X[J', :] Y[:, J'] for the next block J' = [b0, b0 + nb) (nb <= 16)
-__device__ void correct_block(double* G, int ld, const MetroShared& sh, int ldp, int b0, int nb, int a) {
-  const int lane = threadIdx.x & 31;
+// G[0:N, 0:N] += X[:, 0:k] Y[0:k, :] (k <= 16), the flush of one block's flips: 48 x 32
+// warp tiles (3 x 4 DMMA tiles sharing their fragments; 144 = 3 x 48), all warps
+__device__ void flush_block(double* G, int ld, int N, const double* X, int ldx, const double* Y, int ldy, int k) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int g = lane >> 2, q = lane & 3;
-  const int ksteps = (a + 3) >> 2;
+  const int mt = (N + 47) / 48, ns = (N + 31) / 32;
+  const int ksteps = (k + 3) >> 2;
+  for (int st = warp; st < mt * ns; st += nw) {
+    const int r0 = (st % mt) * 48, c0 = (st / mt) * 32;
+    double acc[3][4][4];
 #pragma unroll
-  for (int tn = 0; tn < 2; ++tn) {
-    if (tn * 8 < nb) {
-      double acc[4];
-      const int c = tn * 8 + 2 * q;
-      const bool v00 = g < nb && c < nb, v01 = g < nb && c + 1 < nb;
-      const bool v10 = g + 8 < nb && c < nb, v11 = g + 8 < nb && c + 1 < nb;
-      acc[0] = v00 ? G[b0 + g + (size_t)(b0 + c) * ld] : 0.0;
-      acc[1] = v01 ? G[b0 + g + (size_t)(b0 + c + 1) * ld] : 0.0;
-      acc[2] = v10 ? G[b0 + g + 8 + (size_t)(b0 + c) * ld] : 0.0;
-      acc[3] = v11 ? G[b0 + g + 8 + (size_t)(b0 + c + 1) * ld] : 0.0;
+    for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int s = 0; s < 4; ++s) {
-        if (s < ksteps) {
-          const int m = 4 * s + q;
-          const bool mk = m < a;
-          const double a0 = (g < nb && mk) ? sh.X[b0 + g + m * ldp] : 0.0;
-          const double a1 = (g + 8 < nb && mk) ? sh.X[b0 + g + 8 + m * ldp] : 0.0;
-          const double b0v = (tn * 8 + g < nb && mk) ? sh.Y[m * ldp + b0 + tn * 8 + g] : 0.0;
-          dmma_16x8x4(acc, a0, a1, b0v);
-        }
+      for (int t = 0; t < 4; ++t) {
+        const int r = r0 + 16 * i + g, c = c0 + t * 8 + 2 * q;
+        acc[i][t][0] = (r < N && c < N) ? G[r + (size_t)c * ld] : 0.0;
+        acc[i][t][1] = (r < N && c + 1 < N) ? G[r + (size_t)(c + 1) * ld] : 0.0;
+        acc[i][t][2] = (r + 8 < N && c < N) ? G[r + 8 + (size_t)c * ld] : 0.0;
+        acc[i][t][3] = (r + 8 < N && c + 1 < N) ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
       }
-      if (v00) G[b0 + g + (size_t)(b0 + c) * ld] = acc[0];
-      if (v01) G[b0 + g + (size_t)(b0 + c + 1) * ld] = acc[1];
-      if (v10) G[b0 + g + 8 + (size_t)(b0 + c) * ld] = acc[2];
-      if (v11) G[b0 + g + 8 + (size_t)(b0 + c + 1) * ld] = acc[3];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      if (s < ksteps) {
+        const int m = 4 * s + q;
+        const bool mk = m < k;
+        double fa[3][2], fb[4];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const int r = r0 + 16 * i + g;
+          fa[i][0] = (r < N && mk) ? X[r + m * ldx] : 0.0;
+          fa[i][1] = (r + 8 < N && mk) ? X[r + 8 + m * ldx] : 0.0;
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int cb = c0 + t * 8 + g;
+          fb[t] = (cb < N && mk) ? Y[m * ldy + cb] : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int t = 0; t < 4; ++t) dmma_16x8x4(acc[i][t], fa[i][0], fa[i][1], fb[t]);
+      }
     }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int r = r0 + 16 * i + g, c = c0 + t * 8 + 2 * q;
+        if (r < N && c < N) G[r + (size_t)c * ld] = acc[i][t][0];
+        if (r < N && c + 1 < N) G[r + (size_t)(c + 1) * ld] = acc[i][t][1];
+        if (r + 8 < N && c < N) G[r + 8 + (size_t)c * ld] = acc[i][t][2];
+        if (r + 8 < N && c + 1 < N) G[r + 8 + (size_t)(c + 1) * ld] = acc[i][t][3];
+      }
   }
-  __syncwarp();
 }
 
 template <int NB>
@@ -390,28 +376,17 @@ __device__ void metropolis_slice_blk(const HqChain& ch, double* G, int ld, const
   rng = minstd_mulmod(minstd_pow(2ull * N), rng);
   __syncthreads();
   double acc_count = 0.0;
-  if (warp == 0) walk_block<NB>(ch, G, ld, sh, 0, min(NB, N), log, 0, acc_count);
   for (int b0 = 0, bi = 0; b0 < N; b0 += NB, ++bi) {
-    // records and factors of block bi are complete; so is the flush of block bi-1
+    if (warp == 0) walk_block<NB>(ch, G, ld, sh, b0, min(NB, N - b0), log, bi & 1, acc_count);
     __syncthreads();
+    // the count alternates between two words: with no flush (a == 0) no barrier follows,
+    // and warp 0 writes the next block's count while other warps may still read this one
     const int a = sh.ired[bi & 1];
-    const int b0n = b0 + NB;
-    const bool next = b0n < N;
-    const int nbn = next ? min(NB, N - b0n) : 0;
-    if (a > 0) {
-      form_panels(G, ld, N, sh, ldp, a);
-      __syncthreads();
-      if (next && warp == 0) {
-        correct_block(G, ld, sh, ldp, b0n, nbn, a);
-        walk_block<NB>(ch, G, ld, sh, b0n, nbn, log, (bi + 1) & 1, acc_count);
-      } else {
-        const int w0 = next ? 1 : 0;
-        rank_update_ex(G, ld, N, N, sh.X, ldp, sh.Y, ldp, a, w0, nwarps - w0, next ? b0n : 0,
-                       next ? b0n + nbn : 0);
-      }
-    } else if (next && warp == 0) {
-      walk_block<NB>(ch, G, ld, sh, b0n, nbn, log, (bi + 1) & 1, acc_count);
-    }
+    if (a == 0) continue;
+    build_panels<NB>(G, ld, N, sh, ldp, a, b0);
+    __syncthreads();
+    flush_block(G, ld, N, sh.X, ldp, sh.Y, ldp, a);
+    __syncthreads();
   }
   __syncthreads();
   n_acc += acc_count;
@@ -438,6 +413,17 @@ __device__ void metropolis_dispatch(const HqChain& ch, double* G, int ld, const 
 // ---------------------------------------------------------------------------------
 __device__ void wrap_slice(const HqChain& ch, double* G, int ld, const int8_t* s, int dir, double* stage) {
   const int N = ch.N;
+  if (ch.expk_mode == HQK_EXPK_SEPARABLE) {
+    // the e^{+-V} scalings ride on the last pass (up) or on the first pass (down)
+    if (dir == HQ_UP) {
+      sep_apply_any(G, ld, N, ch.L, ch.sep_a, ch.sep_c, 0);
+      sep_apply_any<0, 2>(G, ld, N, ch.L, ch.sep_ai, ch.sep_ci, 1, s, ch.ev_p, ch.ev_m, ch.ev_m, ch.ev_p);
+    } else {
+      sep_apply_any<1, 0>(G, ld, N, ch.L, ch.sep_ai, ch.sep_ci, 0, s, ch.ev_m, ch.ev_p, ch.ev_p, ch.ev_m);
+      sep_apply_any(G, ld, N, ch.L, ch.sep_a, ch.sep_c, 1);
+    }
+    return;
+  }
   if (dir == HQ_UP) {
     apply_expk(ch, G, ld, 0, false, stage);
     apply_expk(ch, G, ld, 1, true, stage);
@@ -513,13 +499,12 @@ k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int 
   sh.ired = ired;
   __shared__ int qj_s[16];
   __shared__ double qg_s[16];
-  __shared__ double xl_s[16 * 16], yl_s[16 * 16], am_s[16 * 16], bm_s[16 * 16];
+  __shared__ __align__(16) double xt_s[16 * 16];
+  __shared__ __align__(16) double yt_s[16 * 16];
   sh.qj = qj_s;
   sh.qg = qg_s;
-  sh.xl = xl_s;
-  sh.yl = yl_s;
-  sh.Am = am_s;
-  sh.Bm = bm_s;
+  sh.xt = xt_s;
+  sh.yt = yt_s;
   uint32_t rng = *ch.rng;
   double n_acc = 0.0, n_prop = 0.0;
   long long log_base = (flags & HQ_F_LOG_RATIOS) && ch.ratio_count ? *ch.ratio_count : 0;
@@ -661,6 +646,82 @@ __device__ void qr_panel(double* A, int ld, int N, int p0, int p1, double* tau) 
   }
 }
 
+// reflector of column c (dlarfg convention) by the warp that holds the column in registers
+// (x[t] = A[lane + 32 t, c]); writes the column (R entries, beta, v) and tau[c]
+template <int RPL>
+__device__ __forceinline__ void reflector_reg(double* A, int ld, int N, int c, double (&x)[RPL], double* tau) {
+  const int lane = threadIdx.x & 31;
+  double xs = 0.0, alpha = 0.0;
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) {
+    const int r = lane + 32 * t;
+    if (r > c && r < N) xs = fma(x[t], x[t], xs);
+    if (r == c) alpha = x[t];
+  }
+  xs = warp_sum(xs);
+  alpha = __shfl_sync(0xffffffffu, alpha, c & 31);
+  double ti = 0.0, beta = alpha;
+  if (xs > 0.0) {
+    beta = -copysign(hypot(alpha, sqrt(xs)), alpha);
+    ti = (beta - alpha) / beta;
+    const double sc = 1.0 / (alpha - beta);
+#pragma unroll
+    for (int t = 0; t < RPL; ++t) {
+      const int r = lane + 32 * t;
+      if (r > c && r < N) x[t] *= sc;
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) {
+    const int r = lane + 32 * t;
+    if (r == c) x[t] = beta;
+    if (r < N) A[r + (size_t)c * ld] = x[t];
+  }
+  if (lane == 0) tau[c] = ti;
+}
+
+// Householder QR of the panel columns [p0, p1) for N <= 32 RPL: warp j holds column p0 + j in
+// registers; the owner of column c+1 forms reflector c+1 right after applying reflector c,
+// so one block barrier separates consecutive reflectors
+template <int RPL>
+__device__ void qr_panel_reg(double* A, int ld, int N, int p0, int p1, double* tau) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int col = p0 + warp;
+  const bool own = col < p1;
+  double x[RPL];
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) {
+    const int r = lane + 32 * t;
+    x[t] = (own && r < N) ? A[r + (size_t)col * ld] : 0.0;
+  }
+  if (warp == 0) reflector_reg<RPL>(A, ld, N, p0, x, tau);
+  __syncthreads();
+  for (int c = p0; c + 1 < p1; ++c) {
+    if (own && col > c) {
+      const double ti = tau[c];
+      if (ti != 0.0) {
+        double v[RPL];
+        double w = 0.0;
+#pragma unroll
+        for (int t = 0; t < RPL; ++t) {
+          const int r = lane + 32 * t;
+          v[t] = (r > c && r < N) ? A[r + (size_t)c * ld] : 0.0;
+          w = (r == c) ? w + x[t] : fma(v[t], x[t], w);
+        }
+        w = warp_sum(w) * ti;
+#pragma unroll
+        for (int t = 0; t < RPL; ++t) {
+          const int r = lane + 32 * t;
+          if (r == c) x[t] -= w;
+          else x[t] = fma(-w, v[t], x[t]);
+        }
+      }
+      if (col == c + 1) reflector_reg<RPL>(A, ld, N, c + 1, x, tau);
+    }
+    __syncthreads();
+  }
+}
+
 // V of the panel [p0, p0+m) with explicit unit diagonal and zeros above (columns >= m
 // zero), and the triangular factor T of H_p0 ... H_p0+m-1 = I - V T V^T
 __device__ void wy_factor(const double* A, int ld, int N, int p0, int m, const double* tau, double* Vb, int ldv,
@@ -671,31 +732,53 @@ __device__ void wy_factor(const double* A, int ld, int N, int p0, int m, const d
       Vb[r + q * ldv] = (q >= m || r < c) ? 0.0 : (r == c ? 1.0 : A[r + (size_t)c * ld]);
     }
   __syncthreads();
-  // S = V^T V (upper triangle), rows >= p0 + b are the only nonzero overlap
-  for (int t = threadIdx.x; t < kQB * kQB; t += blockDim.x) {
-    const int a = t / kQB, bb = t % kQB;
-    double acc = 0.0;
-    if (a <= bb && bb < m)
-      for (int r = p0 + bb; r < N; ++r) acc = fma(Vb[r + a * ldv], Vb[r + bb * ldv], acc);
-    S[t] = acc;
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    const int i = threadIdx.x;
-    for (int j = 0; j < kQB; ++j) {
-      if (i < kQB) {
-        double v = 0.0;
-        if (j < m) {
-          if (i == j) v = tau[p0 + j];
-          else if (i < j) {
-            double acc = 0.0;
-            for (int l = i; l < j; ++l) acc = fma(T[i * kQB + l], S[l * kQB + j], acc);
-            v = -tau[p0 + j] * acc;
-          }
-        }
-        T[i * kQB + j] = v;
+  // S = V^T V on DMMA: warps 0 / 1 take output columns 0-7 / 8-15, four accumulator chains
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  if (warp < 2) {
+    const int n0 = warp * 8;
+    double acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
+    for (int r0 = p0; r0 < N; r0 += 16) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int r = r0 + 4 * u + q;
+        const bool ok = r < N;
+        const double a0 = ok ? Vb[r + g * ldv] : 0.0;
+        const double a1 = ok ? Vb[r + (g + 8) * ldv] : 0.0;
+        const double b0 = ok ? Vb[r + (n0 + g) * ldv] : 0.0;
+        dmma_16x8x4(acc[u], a0, a1, b0);
       }
     }
+    const int cc = n0 + 2 * q;
+    S[g * kQB + cc] = (acc[0][0] + acc[1][0]) + (acc[2][0] + acc[3][0]);
+    S[g * kQB + cc + 1] = (acc[0][1] + acc[1][1]) + (acc[2][1] + acc[3][1]);
+    S[(g + 8) * kQB + cc] = (acc[0][2] + acc[1][2]) + (acc[2][2] + acc[3][2]);
+    S[(g + 8) * kQB + cc + 1] = (acc[0][3] + acc[1][3]) + (acc[2][3] + acc[3][3]);
+  }
+  __syncthreads();
+  // T[i][j] = -tau_j sum_{i <= l < j} T[i][l] S[l][j] (T[i][i] = tau_i): lane i keeps row i
+  if (warp == 0 && lane < kQB) {
+    const int i = lane;
+    double t[kQB];
+#pragma unroll
+    for (int j = 0; j < kQB; ++j) {
+      double v = 0.0;
+      if (j < m) {
+        if (i == j) {
+          v = tau[p0 + j];
+        } else if (i < j) {
+          double acc = 0.0;  // t[l] = 0 for l < i
+#pragma unroll
+          for (int l = 0; l < j; ++l) acc = fma(t[l], S[l * kQB + j], acc);
+          v = -tau[p0 + j] * acc;
+        }
+      }
+      t[j] = v;
+    }
+#pragma unroll
+    for (int j = 0; j < kQB; ++j) T[i * kQB + j] = t[j];
   }
   __syncthreads();
 }
@@ -705,35 +788,48 @@ __device__ void wy_apply(double* A, int ld, int N, int p0, const double* Vb, int
                          double* W, int ldw, int col0, int nc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int g = lane >> 2, q = lane & 3;
-  // W = V^T A_sub (kQB x nc) with DMMA: m16 = the panel columns, k = rows p0..N-1
+  // W = V^T A_sub (kQB x nc) with DMMA: m16 = the panel columns, k = rows p0..N-1, four
+  // accumulator chains per 8-column tile
   const int nt8 = (nc + 7) / 8;
   for (int t = warp; t < nt8; t += nwarps) {
     const int cb = t * 8 + g;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int r0 = p0; r0 < N; r0 += 4) {
-      const int r = r0 + q;
-      const double a0 = (r < N) ? Vb[r + g * ldv] : 0.0;
-      const double a1 = (r < N) ? Vb[r + (g + 8) * ldv] : 0.0;
-      const double b0 = (r < N && cb < nc) ? A[r + (size_t)(col0 + cb) * ld] : 0.0;
-      dmma_16x8x4(acc, a0, a1, b0);
+    double acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
+    for (int r0 = p0; r0 < N; r0 += 16) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int r = r0 + 4 * u + q;
+        const double a0 = (r < N) ? Vb[r + g * ldv] : 0.0;
+        const double a1 = (r < N) ? Vb[r + (g + 8) * ldv] : 0.0;
+        const double b0 = (r < N && cb < nc) ? A[r + (size_t)(col0 + cb) * ld] : 0.0;
+        dmma_16x8x4(acc[u], a0, a1, b0);
+      }
     }
     const int c = t * 8 + 2 * q;
-    if (c < nc) { W[g * ldw + c] = acc[0]; W[(g + 8) * ldw + c] = acc[2]; }
-    if (c + 1 < nc) { W[g * ldw + c + 1] = acc[1]; W[(g + 8) * ldw + c + 1] = acc[3]; }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[0][e] = (acc[0][e] + acc[1][e]) + (acc[2][e] + acc[3][e]);
+    if (c < nc) { W[g * ldw + c] = acc[0][0]; W[(g + 8) * ldw + c] = acc[0][2]; }
+    if (c + 1 < nc) { W[g * ldw + c + 1] = acc[0][1]; W[(g + 8) * ldw + c + 1] = acc[0][3]; }
   }
   __syncthreads();
-  // W <- -op(T) W, one thread per column
-  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
-    double w[kQB];
+  // W <- -op(T) W by DMMA, in place per 8-column tile (a tile's loads precede its stores)
+  for (int t = warp; t < nt8; t += nwarps) {
+    const int n = t * 8 + g;
+    double bw[4];
 #pragma unroll
-    for (int l = 0; l < kQB; ++l) w[l] = W[l * ldw + c];
+    for (int s4 = 0; s4 < 4; ++s4) bw[s4] = (n < nc) ? W[(4 * s4 + q) * ldw + n] : 0.0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int i = 0; i < kQB; ++i) {
-      double acc = 0.0;
-#pragma unroll
-      for (int l = 0; l < kQB; ++l) acc = fma(trans ? T[l * kQB + i] : T[i * kQB + l], w[l], acc);
-      W[i * ldw + c] = -acc;
+    for (int s4 = 0; s4 < 4; ++s4) {
+      const int l = 4 * s4 + q;
+      const double a0 = trans ? T[l * kQB + g] : T[g * kQB + l];
+      const double a1 = trans ? T[l * kQB + g + 8] : T[(g + 8) * kQB + l];
+      dmma_16x8x4(acc, a0, a1, bw[s4]);
     }
+    const int c = t * 8 + 2 * q;
+    if (c < nc) { W[g * ldw + c] = -acc[0]; W[(g + 8) * ldw + c] = -acc[2]; }
+    if (c + 1 < nc) { W[g * ldw + c + 1] = -acc[1]; W[(g + 8) * ldw + c + 1] = -acc[3]; }
   }
   __syncthreads();
   // A_sub += V (-op(T) W)
@@ -790,7 +886,8 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
   // ---- blocked Householder QR ----
   for (int p0 = 0; p0 < N; p0 += kQB) {
     const int p1 = min(p0 + kQB, N);
-    qr_panel(A, ld, N, p0, p1, tau);
+    if (N <= 160) qr_panel_reg<5>(A, ld, N, p0, p1, tau);
+    else qr_panel(A, ld, N, p0, p1, tau);
     if (p1 < N) {
       wy_factor(A, ld, N, p0, p1 - p0, tau, Vb, ldp, T, S);
       wy_apply(A, ld, N, p0, Vb, ldp, T, true, W, ldp, p1, N - p1);
@@ -811,30 +908,27 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
     Tout[r + (size_t)order[cc] * N] = (nrm[r] != 0.0) ? v : (r == cc ? 1.0 : 0.0);
   }
   __syncthreads();
-  // ---- form Q in place, panels backwards ----
+  // ---- form Q in place, panels backwards: the trailing columns get the panel's WY
+  // transformation, the panel's own columns (identity columns until now) are in closed form
+  //   Q[:, p0:p1] = E - V T V[p0:p1, :]^T ----
   for (int p0 = ((N - 1) / kQB) * kQB; p0 >= 0; p0 -= kQB) {
-    const int p1 = min(p0 + kQB, N);
-    if (p1 < N) {
-      wy_factor(A, ld, N, p0, p1 - p0, tau, Vb, ldp, T, S);
-      wy_apply(A, ld, N, p0, Vb, ldp, T, false, W, ldp, p1, N - p1);
+    const int p1 = min(p0 + kQB, N), m = p1 - p0;
+    wy_factor(A, ld, N, p0, m, tau, Vb, ldp, T, S);
+    if (p1 < N) wy_apply(A, ld, N, p0, Vb, ldp, T, false, W, ldp, p1, N - p1);
+    for (int t = threadIdx.x; t < kQB * kQB; t += blockDim.x) {
+      const int l = t / kQB, j = t % kQB;
+      double acc = 0.0;
+      if (j < m)
+        for (int l2 = 0; l2 < kQB; ++l2) acc = fma(T[l * kQB + l2], Vb[(p0 + j) + l2 * ldp], acc);
+      W[l * ldp + j] = -acc;
     }
-    // unblocked formation of the panel's own columns (dorg2r restricted to the panel)
-    for (int i = p1 - 1; i >= p0; --i) {
-      const double ti = tau[i];
-      const int j = i + 1 + warp;
-      if (ti != 0.0 && j < p1) {
-        double w = (lane == 0) ? A[i + (size_t)j * ld] : 0.0;
-        for (int r = i + 1 + lane; r < N; r += 32) w = fma(A[r + (size_t)i * ld], A[r + (size_t)j * ld], w);
-        w = warp_sum(w) * ti;
-        if (lane == 0) A[i + (size_t)j * ld] -= w;
-        for (int r = i + 1 + lane; r < N; r += 32) A[r + (size_t)j * ld] = fma(-w, A[r + (size_t)i * ld], A[r + (size_t)j * ld]);
-      }
-      __syncthreads();
-      for (int r = i + 1 + threadIdx.x; r < N; r += blockDim.x) A[r + (size_t)i * ld] *= -ti;
-      if (threadIdx.x == 0) A[i + (size_t)i * ld] = 1.0 - ti;
-      for (int r = threadIdx.x; r < i; r += blockDim.x) A[r + (size_t)i * ld] = 0.0;
-      __syncthreads();
+    for (int idx = threadIdx.x; idx < N * m; idx += blockDim.x) {
+      const int r = idx % N, j = idx / N;
+      A[r + (size_t)(p0 + j) * ld] = (r == p0 + j) ? 1.0 : 0.0;
     }
+    __syncthreads();
+    rank_update(A + p0 + (size_t)p0 * ld, ld, N - p0, m, Vb + p0, ldp, W, ldp, kQB);
+    __syncthreads();
   }
   double* Uout = ch.stackU + ((size_t)side * ch.n_stab + entry) * NN;
   copy_mat(Uout, N, A, ld, N);
