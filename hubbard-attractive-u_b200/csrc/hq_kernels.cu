@@ -302,12 +302,13 @@ __device__ void build_panels(const double* G, int ld, int N, const MetroShared& 
   }
 }
 
-// G[0:N, 0:N] += X[:, 0:k] Y[0:k, :] (k <= 16), the flush of one block's flips: 48 x 32
-// warp tiles (3 x 4 DMMA tiles sharing their fragments; 144 = 3 x 48), all warps
-__device__ void flush_block(double* G, int ld, int N, const double* X, int ldx, const double* Y, int ldy, int k) {
+// G[0:M, 0:Nc] += X[:, 0:k] Y[0:k, :] (k <= 16): 48 x 32 warp tiles (3 x 4 DMMA tiles sharing
+// their fragments; 144 = 3 x 48), all warps
+__device__ void rank_update48(double* G, int ld, int M, int Nc, const double* X, int ldx, const double* Y, int ldy,
+                              int k) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int g = lane >> 2, q = lane & 3;
-  const int mt = (N + 47) / 48, ns = (N + 31) / 32;
+  const int mt = (M + 47) / 48, ns = (Nc + 31) / 32;
   const int ksteps = (k + 3) >> 2;
   for (int st = warp; st < mt * ns; st += nw) {
     const int r0 = (st % mt) * 48, c0 = (st / mt) * 32;
@@ -317,10 +318,10 @@ __device__ void flush_block(double* G, int ld, int N, const double* X, int ldx, 
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int r = r0 + 16 * i + g, c = c0 + t * 8 + 2 * q;
-        acc[i][t][0] = (r < N && c < N) ? G[r + (size_t)c * ld] : 0.0;
-        acc[i][t][1] = (r < N && c + 1 < N) ? G[r + (size_t)(c + 1) * ld] : 0.0;
-        acc[i][t][2] = (r + 8 < N && c < N) ? G[r + 8 + (size_t)c * ld] : 0.0;
-        acc[i][t][3] = (r + 8 < N && c + 1 < N) ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
+        acc[i][t][0] = (r < M && c < Nc) ? G[r + (size_t)c * ld] : 0.0;
+        acc[i][t][1] = (r < M && c + 1 < Nc) ? G[r + (size_t)(c + 1) * ld] : 0.0;
+        acc[i][t][2] = (r + 8 < M && c < Nc) ? G[r + 8 + (size_t)c * ld] : 0.0;
+        acc[i][t][3] = (r + 8 < M && c + 1 < Nc) ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
       }
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
@@ -331,13 +332,13 @@ __device__ void flush_block(double* G, int ld, int N, const double* X, int ldx, 
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
           const int r = r0 + 16 * i + g;
-          fa[i][0] = (r < N && mk) ? X[r + m * ldx] : 0.0;
-          fa[i][1] = (r + 8 < N && mk) ? X[r + 8 + m * ldx] : 0.0;
+          fa[i][0] = (r < M && mk) ? X[r + m * ldx] : 0.0;
+          fa[i][1] = (r + 8 < M && mk) ? X[r + 8 + m * ldx] : 0.0;
         }
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
           const int cb = c0 + t * 8 + g;
-          fb[t] = (cb < N && mk) ? Y[m * ldy + cb] : 0.0;
+          fb[t] = (cb < Nc && mk) ? Y[m * ldy + cb] : 0.0;
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i)
@@ -350,12 +351,17 @@ __device__ void flush_block(double* G, int ld, int N, const double* X, int ldx, 
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int r = r0 + 16 * i + g, c = c0 + t * 8 + 2 * q;
-        if (r < N && c < N) G[r + (size_t)c * ld] = acc[i][t][0];
-        if (r < N && c + 1 < N) G[r + (size_t)(c + 1) * ld] = acc[i][t][1];
-        if (r + 8 < N && c < N) G[r + 8 + (size_t)c * ld] = acc[i][t][2];
-        if (r + 8 < N && c + 1 < N) G[r + 8 + (size_t)(c + 1) * ld] = acc[i][t][3];
+        if (r < M && c < Nc) G[r + (size_t)c * ld] = acc[i][t][0];
+        if (r < M && c + 1 < Nc) G[r + (size_t)(c + 1) * ld] = acc[i][t][1];
+        if (r + 8 < M && c < Nc) G[r + 8 + (size_t)c * ld] = acc[i][t][2];
+        if (r + 8 < M && c + 1 < Nc) G[r + 8 + (size_t)(c + 1) * ld] = acc[i][t][3];
       }
   }
+}
+
+// the flush of one block's flips, G[0:N, 0:N] += X[:, 0:k] Y[0:k, :]
+__device__ void flush_block(double* G, int ld, int N, const double* X, int ldx, const double* Y, int ldy, int k) {
+  rank_update48(G, ld, N, N, X, ldx, Y, ldy, k);
 }
 
 template <int NB>
@@ -1072,11 +1078,7 @@ k_invert(const HqChain* __restrict__ chains, int nchains, int b, int which, int 
   }
 }
 
-// ---------------------------------------------------------------------------------
-//  k_gemm: batched C = alpha * op(A) diag(f(ks)) op(B) * rowscale * colscale + beta C.
-//  64 x 64 output tile per CTA, 4 warps (each 32 x 32 = 2 x 4 DMMA m16n8k4 tiles),
-//  k-chunks of 16 staged in shared memory.
-// ---------------------------------------------------------------------------------
+// scaling of index i: 1 (mode 0 or no vector), v[i] (1), 1 / max(v[i], 1) (2), min(v[i], 1) (3)
 __device__ __forceinline__ double vscale(const double* v, int mode, int i) {
   if (!v || mode == 0) return 1.0;
   const double x = v[i];
