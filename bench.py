@@ -184,11 +184,14 @@ def fp64_peak_tflops(torch, device):
 
 def interval_flops(nl, n_slices, accepted, kmax, expk_mode):
     """Algorithmic FP64 flops of the interval kernel: wraps of n_slices slices plus
-    `accepted` Sherman-Morrison flips in delayed rank-k form."""
+    `accepted` flips in submatrix form (blocks of kmax sites): per flip the rank-1 share of
+    the DMMA flush (2 N^2) and its panel row / column (4 N m for the m-th flip of a block)."""
     N = nl * nl
     wrap = (8.0 * N * nl ** 3) if expk_mode == 1 else (4.0 * N ** 3)  # two expK applications per slice
-    kbar = (kmax - 1) / 2.0
-    flip = 2.0 * N * N + 4.0 * N * kbar  # rank-1 contribution of the flush + panel build
+    blocks = n_slices * ((N + kmax - 1) // kmax)
+    per_block = accepted / blocks if blocks else 0.0
+    mbar = max(per_block - 1.0, 0.0) / 2.0  # mean in-block index of an accepted flip
+    flip = 2.0 * N * N + 4.0 * N * mbar
     return n_slices * wrap + accepted * flip
 
 
