@@ -200,7 +200,7 @@ __device__ inline void sep_apply(double* M, int ld, int N, const double* a, doub
 
 // dispatch on the lattice size to an exact compile-time fiber length (L <= HQ_MAX_L)
 template <int SC0 = 0, int SC1 = 0>
-__device__ inline void sep_apply_any(double* M, int ld, int N, int L, const double* a, double c, int side,
+__device__ __forceinline__ void sep_apply_any(double* M, int ld, int N, int L, const double* a, double c, int side,
                                      const int8_t* sf = nullptr, double rp = 1.0, double rm = 1.0,
                                      double cp = 1.0, double cm = 1.0) {
   switch (L) {

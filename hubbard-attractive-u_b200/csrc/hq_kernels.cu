@@ -57,7 +57,7 @@ struct SliceView {
 //  filling = 2 - 2 trG/N ; docc = sum_i (1-G_ii)^2 / N ;
 //  swave   = sum_ij [(1-G)_ji^2 + G_ij^2] / N = (2 sum G^2 - 2 trG + N) / N
 // ---------------------------------------------------------------------------------
-__device__ void measure_slice(const double* G, int ld, int N, double* acc, double* red) {
+__device__ __forceinline__ void measure_slice(const double* G, int ld, int N, double* acc, double* red) {
   double tr = 0.0, dd = 0.0, sq = 0.0;
   HQ_FOR_EACH_ELEM(N, i, j) {
     const double v = G[i + (size_t)j * ld];
@@ -73,7 +73,7 @@ __device__ void measure_slice(const double* G, int ld, int N, double* acc, doubl
   }
 }
 
-__device__ void copy_mat(double* dst, int ldd, const double* src, int lds, int N) {
+__device__ __forceinline__ void copy_mat(double* dst, int ldd, const double* src, int lds, int N) {
   HQ_FOR_EACH_ELEM(N, i, j) dst[i + (size_t)j * ldd] = src[i + (size_t)j * lds];
 }
 
@@ -175,7 +175,7 @@ struct MetroShared {
 // the walk of the block [b0, b0 + nb) by one warp (see above); writes the records, the
 // accepted count into ired[slot] and the two triangular factors
 template <int NB>
-__device__ void walk_block(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0, int nb,
+__device__ __forceinline__ void walk_block(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0, int nb,
                            bool log, int slot, double& acc_count) {
   constexpr int R = (NB * NB >= 32) ? NB * NB / 32 : 1;  // rows of g held by one lane
   constexpr int H = NB / R;                              // lane groups (rows h*R .. h*R+R-1)
@@ -261,7 +261,7 @@ __device__ void walk_block(const HqChain& ch, const double* G, int ld, const Met
 // and one column of Y per thread; the coefficients of flip m are contiguous in the records
 // (xt / yt at row j_m - b0) and are read in 16-byte pairs
 template <int NB>
-__device__ void build_panels(const double* G, int ld, int N, const MetroShared& sh, int ldp, int a, int b0) {
+__device__ __forceinline__ void build_panels(const double* G, int ld, int N, const MetroShared& sh, int ldp, int a, int b0) {
   for (int p = threadIdx.x; p < N; p += blockDim.x) {
     double x[NB], y[NB];
 #pragma unroll
@@ -304,7 +304,7 @@ __device__ void build_panels(const double* G, int ld, int N, const MetroShared& 
 
 // G[0:M, 0:Nc] += X[:, 0:k] Y[0:k, :] (k <= 16): 48 x 32 warp tiles (3 x 4 DMMA tiles sharing
 // their fragments; 144 = 3 x 48), all warps
-__device__ void rank_update48(double* G, int ld, int M, int Nc, const double* X, int ldx, const double* Y, int ldy,
+__device__ __forceinline__ void rank_update48(double* G, int ld, int M, int Nc, const double* X, int ldx, const double* Y, int ldy,
                               int k) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int g = lane >> 2, q = lane & 3;
@@ -360,12 +360,12 @@ __device__ void rank_update48(double* G, int ld, int M, int Nc, const double* X,
 }
 
 // the flush of one block's flips, G[0:N, 0:N] += X[:, 0:k] Y[0:k, :]
-__device__ void flush_block(double* G, int ld, int N, const double* X, int ldx, const double* Y, int ldy, int k) {
+__device__ __forceinline__ void flush_block(double* G, int ld, int N, const double* X, int ldx, const double* Y, int ldy, int k) {
   rank_update48(G, ld, N, N, X, ldx, Y, ldy, k);
 }
 
 template <int NB>
-__device__ void metropolis_slice_blk(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
+__device__ __forceinline__ void metropolis_slice_blk(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
                                      double& n_acc, int flags, long long log_base) {
   const int N = ch.N;
   const int ldp = panel_ld(N);
@@ -405,7 +405,7 @@ __device__ void metropolis_slice_blk(const HqChain& ch, double* G, int ld, const
 }
 
 // block size NB of the submatrix updates: the chain's delay depth (4, 8 or 16)
-__device__ void metropolis_dispatch(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
+__device__ __forceinline__ void metropolis_dispatch(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
                                     double& n_acc, int flags, long long log_base) {
   if (ch.kmax >= 16) metropolis_slice_blk<16>(ch, G, ld, sh, rng, n_acc, flags, log_base);
   else if (ch.kmax >= 8) metropolis_slice_blk<8>(ch, G, ld, sh, rng, n_acc, flags, log_base);
@@ -417,7 +417,7 @@ __device__ void metropolis_dispatch(const HqChain& ch, double* G, int ld, const 
 //   up  : G <- e^{V_l} E G E^{-1} e^{-V_l}
 //   down: G <- E^{-1} e^{-V_l} G e^{V_l} E
 // ---------------------------------------------------------------------------------
-__device__ void wrap_slice(const HqChain& ch, double* G, int ld, const int8_t* s, int dir, double* stage) {
+__device__ __forceinline__ void wrap_slice(const HqChain& ch, double* G, int ld, const int8_t* s, int dir, double* stage) {
   const int N = ch.N;
   if (ch.expk_mode == HQK_EXPK_SEPARABLE) {
     // the e^{+-V} scalings ride on the last pass (up) or on the first pass (down)
@@ -593,7 +593,11 @@ k_bchain(const HqChain* __restrict__ chains, int nchains, int dir, int b, int re
     const int l = t % ch.nt;
     for (int i = threadIdx.x; i < N; i += blockDim.x) s[i] = ch.fields[(size_t)l * N + i];
     __syncthreads();
-    if (dir == HQ_DOWN) {
+    if (ch.expk_mode == HQK_EXPK_SEPARABLE) {
+      // e^{V} rides on the first pass (down: before expK) or the last pass (up: after it)
+      if (dir == HQ_DOWN) sep_apply_any<1, 0>(X, ld, N, ch.L, ch.sep_a, ch.sep_c, 0, s, ch.ev_p, ch.ev_m, 1.0, 1.0);
+      else sep_apply_any<0, 2>(X, ld, N, ch.L, ch.sep_a, ch.sep_c, 0, s, ch.ev_p, ch.ev_m, 1.0, 1.0);
+    } else if (dir == HQ_DOWN) {
       scale_rows(X, ld, N, s, ch.ev_p, ch.ev_m);
       __syncthreads();
       apply_expk(ch, X, ld, 0, false, stage);
