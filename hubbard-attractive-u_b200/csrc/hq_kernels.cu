@@ -959,6 +959,111 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
 // ---------------------------------------------------------------------------------
 constexpr int kGJ = 16;
 
+// x[r / 32] (r warp-uniform) without an indexed access: written as a C++ select chain the
+// compiler folds it back into x[r / 32], which moves x to local memory; selp keeps it in
+// registers
+template <int RPL>
+__device__ __forceinline__ double slot_at(const double (&x)[RPL], int r) {
+  const int t = r >> 5;
+  double v = 0.0;
+#pragma unroll
+  for (int i = 0; i < RPL; ++i)
+    asm("{\n\t.reg .pred p;\n\tsetp.eq.s32 p, %2, %3;\n\tselp.f64 %0, %1, %0, p;\n\t}" : "+d"(v) : "d"(x[i]), "r"(t), "r"(i));
+  return v;
+}
+
+// pivot k of a register-resident Gauss-Jordan panel, by the warp that holds column k:
+// partial pivoting (largest |A[r][k]|, r >= k, smallest index among equals), row swap in
+// this column, the multipliers into fcol, the inverse's column k into x, and perm / pinv
+template <int RPL>
+__device__ __forceinline__ void gj_pivot_reg(double (&x)[RPL], int k, int N, double* fcol, double* pinv_out,
+                                             int* perm, double* status) {
+  const int lane = threadIdx.x & 31;
+  double best = -1.0;
+  int bi = N;
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) {
+    const int r = lane + 32 * t;
+    if (r >= k && r < N) {
+      const double v = fabs(x[t]);
+      if (v > best || (v == best && r < bi)) { best = v; bi = r; }
+    }
+  }
+  // warp argmax with three redux steps on the bit pattern of |x| (monotonic for non-negative
+  // doubles; NaNs were skipped by the lane-local search): the high word, then the low word
+  // among the lanes holding the maximum, then the smallest row among those
+  {
+    const unsigned long long bb = best < 0.0 ? 0ull : (unsigned long long)__double_as_longlong(best);
+    const unsigned hi = (unsigned)(bb >> 32), lo = (unsigned)bb;
+    const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+    bi = (int)__reduce_min_sync(0xffffffffu, (hi == mh && lo == ml) ? (unsigned)bi : 0xffffffffu);
+    best = __longlong_as_double((long long)(((unsigned long long)mh << 32) | ml));
+  }
+  const double vk = __shfl_sync(0xffffffffu, slot_at<RPL>(x, k), k & 31);
+  const double vb = __shfl_sync(0xffffffffu, slot_at<RPL>(x, bi), bi & 31);
+  const bool ok = (best > 0.0) && isfinite(best);
+  const double pinv = ok ? 1.0 / vb : 0.0;
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) {
+    const int r = lane + 32 * t;
+    double v = (r == k) ? vb : ((r == bi) ? vk : x[t]);
+    if (r < N) fcol[r] = v;
+    x[t] = (r == k) ? pinv : -v * pinv;
+  }
+  if (lane == 0) {
+    perm[k] = bi;
+    *pinv_out = pinv;
+    if (!ok) *status = 1.0;
+  }
+}
+
+// Gauss-Jordan on the panel columns [p0, p0 + nb) of A (all rows), N <= 32 RPL: warp j holds
+// column p0 + j in registers; the owner of column k+1 takes pivot k+1 right after its own
+// elimination step for pivot k, so one block barrier separates pivots. Multipliers and the
+// reciprocal pivot are double-buffered by pivot parity (fcol: 2N doubles, pv: 2).
+template <int RPL>
+__device__ void gj_panel_reg(double* A, int ld, int N, int p0, int nb, int* perm, double* fcol, double* pv,
+                             double* status) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool own = warp < nb;
+  const int col = p0 + warp;
+  double x[RPL];
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) {
+    const int r = lane + 32 * t;
+    x[t] = (own && r < N) ? A[r + (size_t)col * ld] : 0.0;
+  }
+  if (warp == 0) gj_pivot_reg<RPL>(x, p0, N, fcol, pv, perm, status);
+  __syncthreads();
+  for (int q = 0; q < nb; ++q) {
+    const int k = p0 + q, par = q & 1;
+    if (own && warp != q) {
+      const int bi = perm[k];
+      const double pinv = pv[par];
+      const double* f = fcol + par * N;
+      // row swap k <-> bi in this column, then row k scaled by the pivot's reciprocal
+      const double vk = __shfl_sync(0xffffffffu, slot_at<RPL>(x, k), k & 31);
+      const double vb = __shfl_sync(0xffffffffu, slot_at<RPL>(x, bi), bi & 31);
+      const double u = vb * pinv;
+#pragma unroll
+      for (int t = 0; t < RPL; ++t) {
+        const int r = lane + 32 * t;
+        const double v = (r == bi) ? vk : x[t];
+        x[t] = (r == k) ? u : ((r < N) ? fma(-f[r < N ? r : 0], u, v) : v);
+      }
+      if (warp == q + 1 && q + 1 < nb) gj_pivot_reg<RPL>(x, k + 1, N, fcol + (par ^ 1) * N, pv + (par ^ 1), perm, status);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) {
+    const int r = lane + 32 * t;
+    if (own && r < N) A[r + (size_t)col * ld] = x[t];
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(HQ_THREADS, 1)
 k_invert(const HqChain* __restrict__ chains, int nchains, int b, int which, int resident) {
   extern __shared__ __align__(16) double smem[];
@@ -980,11 +1085,14 @@ k_invert(const HqChain* __restrict__ chains, int nchains, int b, int which, int 
   double* Bf = p; p += (size_t)ldp * kGJ;   // kGJ x N, row-major
   int* perm = reinterpret_cast<int*>(p);
   int* gidx = perm + N;
+  double* fcol = reinterpret_cast<double*>(gidx + N);  // 2 N multipliers (register panel)
+  __shared__ double pv[2];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __syncthreads();
   for (int p0 = 0; p0 < N; p0 += kGJ) {
     const int nb = min(kGJ, N - p0);
-    for (int q = 0; q < nb; ++q) {
+    if (N <= 160) gj_panel_reg<5>(A, ld, N, p0, nb, perm, fcol, pv, ch.acc + HQ_ACC_STATUS);
+    else for (int q = 0; q < nb; ++q) {
       const int k = p0 + q;
       if (warp == 0) {
         // pivot search in column k over rows k..N-1, swap within the panel, scale the pivot row
@@ -1524,7 +1632,7 @@ size_t smem_udt_bytes(int Nmax, bool resident) {
   return smem_matrix_bytes(Nmax, resident, 2 * kQB * panel_ld(Nmax) + 2 * kQB * kQB + 3 * Nmax + 64);
 }
 size_t smem_invert_bytes(int Nmax, bool resident) {
-  return smem_matrix_bytes(Nmax, resident, 2 * kGJ * panel_ld(Nmax) + Nmax + 64);
+  return smem_matrix_bytes(Nmax, resident, 2 * kGJ * panel_ld(Nmax) + 3 * Nmax + 64);
 }
 size_t smem_matrix_bytes(int Nmax, bool resident, int extra_doubles) {
   const size_t mat = resident ? (size_t)Nmax * smem_ld(Nmax) : 0;
