@@ -215,6 +215,8 @@ def run_gpu(args):
     eng = hq.Engine(chain_params(rank, n), device=local)
     eng.fields_random()
     eng.init()
+    # expK application and delay depth picked by timing (the chains' state is restored)
+    tune = [] if args.no_tune else eng.autotune(sweeps=1)
     expk_mode, kmax = eng.config(0)
     stream = torch.cuda.ExternalStream(eng.stream())
     # warm-up: W directional sweeps (alternating), then capture one graph per direction
@@ -355,6 +357,9 @@ def run_gpu(args):
                                    "estimators), 12x12 lattice, beta=10, dt=0.1, nt=100, pace 10",
                        "chains_per_gpu": n, **CFG, "expk_mode": "separable" if expk_mode == 1 else "dense",
                        "delay_depth": kmax, "cuda_graph": True,
+                       "autotune": [{"expk": "separable" if t["expk_mode"] == 1 else "dense", "k": t["delay_depth"],
+                                     "ms_per_sweep": round(t["ms_per_sweep"], 3), "chosen": t["chosen"]}
+                                    for t in tune],
                        "l2": "working set per GPU ~1.8 GB of chain state (> 126 MB L2)"},
             "roofline": roofline,
             "cpu_baseline": cpu,
@@ -388,6 +393,7 @@ def main():
     ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak probe")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-single", action="store_true", help="skip the single-chain leg")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (largest delay depth, separable expK)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

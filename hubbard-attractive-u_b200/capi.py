@@ -26,7 +26,7 @@ EXPORTS = [
     "hq_get_wrap_errors", "hq_get_estimators", "hq_get_dynamic_estimators", "hq_reset_estimators",
     "hq_ratio_log", "hq_logdet_adjoint", "hq_capture_graph", "hq_launch_graph", "hq_get_config",
     "hq_upload_fields_i8", "hq_download_fields_i8", "hq_get_stream", "hq_profile_enable", "hq_profile_collect",
-    "hq_equaltime_g_noalloc",
+    "hq_equaltime_g_noalloc", "hq_autotune",
 ]
 PROFILE_CLASSES = ["interval", "bchain", "udt", "gemm", "invert", "measure", "dynamic", "adjoint"]
 
@@ -45,6 +45,16 @@ class HqChainParams(ctypes.Structure):
         ("delay_depth", ctypes.c_int),
         ("dynamic", ctypes.c_int),
         ("snapshots", ctypes.c_int),
+    ]
+
+
+class HqTuneEntry(ctypes.Structure):
+    _fields_ = [
+        ("nl", ctypes.c_int),
+        ("expk_mode", ctypes.c_int),
+        ("delay_depth", ctypes.c_int),
+        ("ms_per_sweep", ctypes.c_double),
+        ("chosen", ctypes.c_int),
     ]
 
 
@@ -94,6 +104,7 @@ def lib():
             "hq_profile_enable": [vp, c_int],
             "hq_profile_collect": [vp, dp, ctypes.POINTER(c_ll), c_int],
             "hq_equaltime_g_noalloc": [c_int, c_dbl, c_dbl, c_dbl, c_dbl, c_int, c_int, vp, vp, vp],
+            "hq_autotune": [vp, c_int, ctypes.POINTER(HqTuneEntry), c_int, ip],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -241,6 +252,17 @@ class Engine:
         m, k = ctypes.c_int(0), ctypes.c_int(0)
         check(lib().hq_get_config(self.h, chain, ctypes.byref(m), ctypes.byref(k)))
         return m.value, k.value
+
+    def autotune(self, sweeps=2):
+        """Times every (expK mode, delay depth) candidate per lattice size on whole sweeps and
+        keeps the fastest; the chains' state is restored after each candidate. Returns the
+        timed candidates as dicts."""
+        cap = 64
+        buf = (HqTuneEntry * cap)()
+        n = ctypes.c_int(0)
+        check(lib().hq_autotune(self.h, int(sweeps), buf, cap, ctypes.byref(n)))
+        return [dict(nl=e.nl, expk_mode=e.expk_mode, delay_depth=e.delay_depth, ms_per_sweep=e.ms_per_sweep,
+                     chosen=bool(e.chosen)) for e in buf[:min(n.value, cap)]]
 
     def stream(self):
         s = ctypes.c_void_p()

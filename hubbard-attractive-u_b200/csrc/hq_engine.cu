@@ -778,6 +778,19 @@ int hq_init_stacks_and_g(hq_ctx* c) {
   HQ_API_END
 }
 
+// one directional sweep through its captured graph when there is one
+static void dispatch_sweep(hq_ctx* c, int dir, int flags) {
+  auto it = c->graphs.find({dir, flags});
+  if (it != c->graphs.end()) {
+    HQ_CUDA(cudaGraphLaunch(it->second, c->stream));
+    c->prof_next = c->graph_prof[{dir, flags}];
+  } else {
+    issue_sweep(c, dir, flags);
+  }
+  c->at_zero = (dir == HQ_SWEEP_DOWN);
+  c->at_beta = !c->at_zero;
+}
+
 int hq_sweep(hq_ctx* c, int dir, int flags) {
   HQ_API_BEGIN
   if (!c) throw HqError(HQ_E_INVALID, "null context");
@@ -794,15 +807,7 @@ int hq_sweep(hq_ctx* c, int dir, int flags) {
     for (auto& h : c->ch)
       if (!h.p.dynamic) throw HqError(HQ_E_INVALID, "every chain needs dynamic storage for a dynamic sweep");
   }
-  auto it = c->graphs.find({dir, flags});
-  if (it != c->graphs.end()) {
-    HQ_CUDA(cudaGraphLaunch(it->second, c->stream));
-    c->prof_next = c->graph_prof[{dir, flags}];
-  } else {
-    issue_sweep(c, dir, flags);
-  }
-  c->at_zero = (dir == HQ_SWEEP_DOWN);
-  c->at_beta = !c->at_zero;
+  dispatch_sweep(c, dir, flags);
   HQ_API_END
 }
 
@@ -999,6 +1004,91 @@ int hq_get_config(hq_ctx* c, int chain, int* expk_mode, int* delay_depth) {
   check_chain(c, chain);
   if (expk_mode) *expk_mode = c->desc[chain].expk_mode;
   if (delay_depth) *delay_depth = c->desc[chain].kmax;
+  HQ_API_END
+}
+
+// Picks each lattice size's expK application (separable circulant passes or dense DMMA GEMM)
+// and delay depth (submatrix block size) by timing whole directional sweeps of the context
+// with each candidate. The device state is snapshotted before and restored after every
+// candidate, so the chains continue exactly as if no tuning had run.
+int hq_autotune(hq_ctx* c, int sweeps, hq_tune_entry* entries, int capacity, int* n_entries) {
+  HQ_API_BEGIN
+  if (!c) throw HqError(HQ_E_INVALID, "null context");
+  if (!c->initialised) throw HqError(HQ_E_INVALID, "hq_autotune: call hq_init_stacks_and_g first");
+  if (sweeps < 1 || sweeps > 64) throw HqError(HQ_E_RANGE, "hq_autotune: sweeps must be in [1, 64]");
+  if (capacity < 0 || (capacity > 0 && !entries)) throw HqError(HQ_E_INVALID, "hq_autotune: bad entries buffer");
+  std::map<int, std::vector<int>> groups;  // lattice size -> chains
+  for (int i = 0; i < c->n; ++i) groups[c->ch[i].p.nl].push_back(i);
+  char* snap = nullptr;
+  if (cudaMalloc(&snap, c->arena_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    throw HqError(HQ_E_NOMEM, "hq_autotune: no room for a snapshot of " + std::to_string(c->arena_bytes) + " bytes");
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  const bool z0 = c->at_zero, b0 = c->at_beta;
+  std::vector<hq_tune_entry> out;
+  auto run = [&](int n) {
+    for (int s = 0; s < n; ++s) dispatch_sweep(c, c->at_zero ? HQ_SWEEP_UP : HQ_SWEEP_DOWN, HQ_SWEEP_MEASURE);
+  };
+  auto restore = [&]() {
+    HQ_CUDA(cudaMemcpyAsync(c->arena, snap, c->arena_bytes, cudaMemcpyDeviceToDevice, c->stream));
+    c->at_zero = z0;
+    c->at_beta = b0;
+  };
+  try {
+    HQ_CUDA(cudaEventCreate(&e0));
+    HQ_CUDA(cudaEventCreate(&e1));
+    HQ_CUDA(cudaMemcpyAsync(snap, c->arena, c->arena_bytes, cudaMemcpyDeviceToDevice, c->stream));
+    for (auto& g : groups) {
+      const int nl = g.first;
+      bool sep_ok = nl <= HQ_MAX_L;
+      for (int i : g.second) sep_ok = sep_ok && !c->ch[i].custom_hop;
+      std::vector<int> modes;
+      if (sep_ok) modes.push_back(HQ_EXPK_SEPARABLE);
+      modes.push_back(HQ_EXPK_DENSE);
+      std::vector<int> depths;
+      for (int k : {4, 8, 16})
+        if (k <= c->kmax_max) depths.push_back(k);
+      double best = 1e300;
+      size_t best_at = out.size();
+      for (int mode : modes)
+        for (int k : depths) {
+          for (int i : g.second) { c->desc[i].expk_mode = mode; c->desc[i].kmax = k; }
+          upload_desc(c);
+          run(1);  // warm-up
+          HQ_CUDA(cudaEventRecord(e0, c->stream));
+          run(sweeps);
+          HQ_CUDA(cudaEventRecord(e1, c->stream));
+          HQ_CUDA(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          HQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          restore();
+          hq_tune_entry t;
+          t.nl = nl; t.expk_mode = mode; t.delay_depth = k; t.ms_per_sweep = double(ms) / sweeps; t.chosen = 0;
+          if (t.ms_per_sweep < best) { best = t.ms_per_sweep; best_at = out.size(); }
+          out.push_back(t);
+        }
+      out[best_at].chosen = 1;
+      for (int i : g.second) {
+        c->desc[i].expk_mode = out[best_at].expk_mode;
+        c->desc[i].kmax = out[best_at].delay_depth;
+        c->ch[i].expk_mode = out[best_at].expk_mode;
+        c->ch[i].kmax = out[best_at].delay_depth;
+      }
+    }
+    upload_desc(c);
+    HQ_CUDA(cudaStreamSynchronize(c->stream));
+  } catch (...) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(snap);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(snap);
+  for (int k = 0; k < (int)out.size() && k < capacity; ++k) entries[k] = out[k];
+  if (n_entries) *n_entries = (int)out.size();
   HQ_API_END
 }
 

@@ -369,7 +369,7 @@ __device__ __forceinline__ void metropolis_slice_blk(const HqChain& ch, double* 
                                      double& n_acc, int flags, long long log_base) {
   const int N = ch.N;
   const int ldp = panel_ld(N);
-  const int tid = threadIdx.x, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5;
   const bool log = (flags & HQ_F_LOG_RATIOS) && ch.ratios;
   // uniforms of this slice: site i consumes engine draws 2i+1, 2i+2 after the current state
   for (int i = tid; i < N; i += blockDim.x) {

@@ -167,6 +167,23 @@ HQ_API int hq_profile_collect(hq_ctx* ctx, double* ms, long long* counts, int nc
 /* Per-chain expK mode and delay depth actually in use (after autotuning). */
 HQ_API int hq_get_config(hq_ctx* ctx, int chain, int* expk_mode, int* delay_depth);
 
+/* One timed candidate of hq_autotune. */
+typedef struct {
+  int nl;              /* lattice size of the group of chains */
+  int expk_mode;       /* HQ_EXPK_SEPARABLE or HQ_EXPK_DENSE */
+  int delay_depth;     /* sites per submatrix-update block */
+  double ms_per_sweep; /* device time of one directional sweep of the whole context */
+  int chosen;          /* 1: the candidate now in use for this lattice size */
+} hq_tune_entry;
+
+/* Picks, per lattice size, the expK application (the is_fft choice of the reference's
+ * config, src/hubbard.cpp:38-80, here separable circulant passes vs dense DMMA GEMM) and
+ * the delay depth by timing `sweeps` directional sweeps of the whole context per candidate.
+ * The device state is restored after each candidate: the Markov chains are unaffected.
+ * Needs hq_init_stacks_and_g; allocates one temporary copy of the context's device state.
+ * Writes up to `capacity` entries and the total count to *n_entries. */
+HQ_API int hq_autotune(hq_ctx* ctx, int sweeps, hq_tune_entry* entries, int capacity, int* n_entries);
+
 /* Host <-> device copy of the raw device state of all chains' fields (int8, [chain][nt][N])
  * for end-to-end measurements: one cudaMemcpyAsync each on the context stream. */
 HQ_API int hq_upload_fields_i8(hq_ctx* ctx, const signed char* fields_all);
