@@ -26,7 +26,7 @@ EXPORTS = [
     "hq_get_wrap_errors", "hq_get_estimators", "hq_get_dynamic_estimators", "hq_reset_estimators",
     "hq_ratio_log", "hq_logdet_adjoint", "hq_capture_graph", "hq_launch_graph", "hq_get_config",
     "hq_upload_fields_i8", "hq_download_fields_i8", "hq_get_stream", "hq_profile_enable", "hq_profile_collect",
-    "hq_equaltime_g_noalloc", "hq_autotune",
+    "hq_equaltime_g_noalloc", "hq_autotune", "hq_get_stack",
 ]
 PROFILE_CLASSES = ["interval", "bchain", "udt", "gemm", "invert", "measure", "dynamic", "adjoint"]
 
@@ -105,6 +105,7 @@ def lib():
             "hq_profile_collect": [vp, dp, ctypes.POINTER(c_ll), c_int],
             "hq_equaltime_g_noalloc": [c_int, c_dbl, c_dbl, c_dbl, c_dbl, c_int, c_int, vp, vp, vp],
             "hq_autotune": [vp, c_int, ctypes.POINTER(HqTuneEntry), c_int, ip],
+            "hq_get_stack": [vp, c_int, c_int, ip, dp, dp, dp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -263,6 +264,18 @@ class Engine:
         check(lib().hq_autotune(self.h, int(sweeps), buf, cap, ctypes.byref(n)))
         return [dict(nl=e.nl, expk_mode=e.expk_mode, delay_depth=e.delay_depth, ms_per_sweep=e.ms_per_sweep,
                      chosen=bool(e.chosen)) for e in buf[:min(n.value, cap)]]
+
+    def stack(self, chain, side):
+        """(length, U, D, V) of the top of a chain's left (0) or right (1) UDV stack; the
+        product of all pushes is U diag(D) V^T. U, D, V are None for an empty stack."""
+        N = self._N(chain)
+        n = ctypes.c_int(0)
+        check(lib().hq_get_stack(self.h, chain, side, ctypes.byref(n), None, None, None))
+        if n.value == 0:
+            return 0, None, None, None
+        U, V, D = np.zeros((N, N), order="F"), np.zeros((N, N), order="F"), np.zeros(N)
+        check(lib().hq_get_stack(self.h, chain, side, ctypes.byref(n), _dp(U), _dp(D), _dp(V)))
+        return n.value, U, D, V
 
     def stream(self):
         s = ctypes.c_void_p()

@@ -1007,6 +1007,34 @@ int hq_get_config(hq_ctx* c, int chain, int* expk_mode, int* delay_depth) {
   HQ_API_END
 }
 
+// Top entry of a chain's UDV stack, the product U diag(D) V^T of all its pushes: the
+// reference's SvdStack::MatrixU / SingularValues / MatrixV (include/utils/svd_stack.hpp:83-103).
+// Between whole sweeps the stacks are either at tau = 0 (left empty, right full) or at
+// tau = beta (left full, right empty).
+int hq_get_stack(hq_ctx* c, int chain, int side, int* length, double* U, double* D, double* V) {
+  HQ_API_BEGIN
+  check_chain(c, chain);
+  if (side != 0 && side != 1) throw HqError(HQ_E_INVALID, "hq_get_stack: side is 0 (left) or 1 (right)");
+  if (!c->initialised) throw HqError(HQ_E_INVALID, "hq_get_stack: call hq_init_stacks_and_g first");
+  const HqChain& d = c->desc[chain];
+  const int len = (side == 0) ? (c->at_beta ? d.n_stab : 0) : (c->at_zero ? d.n_stab : 0);
+  if (length) *length = len;
+  if (len > 0 && (U || D || V)) {
+    const int N = d.N;
+    const size_t NN = size_t(N) * N, e = size_t(side) * d.n_stab + (len - 1);
+    HQ_CUDA(cudaStreamSynchronize(c->stream));
+    if (U) HQ_CUDA(cudaMemcpy(U, d.stackU + e * NN, NN * sizeof(double), cudaMemcpyDeviceToHost));
+    if (D) HQ_CUDA(cudaMemcpy(D, d.stackD + e * N, N * sizeof(double), cudaMemcpyDeviceToHost));
+    if (V) {
+      std::vector<double> vt(NN);
+      HQ_CUDA(cudaMemcpy(vt.data(), d.stackVt + e * NN, NN * sizeof(double), cudaMemcpyDeviceToHost));
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) V[i + size_t(j) * N] = vt[j + size_t(i) * N];
+    }
+  }
+  HQ_API_END
+}
+
 // Picks each lattice size's expK application (separable circulant passes or dense DMMA GEMM)
 // and delay depth (submatrix block size) by timing whole directional sweeps of the context
 // with each candidate. The device state is snapshotted before and restored after every

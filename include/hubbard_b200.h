@@ -167,6 +167,14 @@ HQ_API int hq_profile_collect(hq_ctx* ctx, double* ms, long long* counts, int nc
 /* Per-chain expK mode and delay depth actually in use (after autotuning). */
 HQ_API int hq_get_config(hq_ctx* ctx, int chain, int* expk_mode, int* delay_depth);
 
+/* Top of a chain's UDV stack (side 0: left, 1: right), replacing Utils::SvdStack's
+ * StackLength / MatrixU / SingularValues / MatrixV (include/utils/svd_stack.hpp:78-103):
+ * *length entries; the product of all pushes is U diag(D) V^T (U: N*N column-major, D: N,
+ * V: N*N, V = the reference's product V_0 V_1 ...). D holds |diag R| of the pre-pivoted QR
+ * that replaces the SVD. Any of U, D, V may be NULL; nothing is written when *length = 0.
+ * Between sweeps the stacks are at tau = 0 (left empty) or at tau = beta (right empty). */
+HQ_API int hq_get_stack(hq_ctx* ctx, int chain, int side, int* length, double* U, double* D, double* V);
+
 /* One timed candidate of hq_autotune. */
 typedef struct {
   int nl;              /* lattice size of the group of chains */

@@ -2,6 +2,7 @@
 // the call surface of the reference's DQMC sweep (JefferyWangSH/hubbard-attractive-U):
 //   DQMC::Core                (include/dqmc_core.h:35-112)
 //   Model::HubbardAttractiveU (include/hubbard.h:32-112)
+//   Utils::SvdStack           (include/utils/svd_stack.hpp:51-190, read-only view)
 //   DQMC::Params              (include/dqmc_params.hpp:20-45)
 // inside namespace hq_b200 so that it can sit next to the reference's own classes. A driver
 // written against the reference (src/dqmc_handle.cpp, src/main.cpp) compiles against these
@@ -88,6 +89,38 @@ class HubbardAttractiveU {
 };
 
 }  // namespace Model
+
+namespace Utils {
+
+// Utils::SvdStack (include/utils/svd_stack.hpp:51-190): a read-only view of the top of one
+// chain's left (side 0) or right (side 1) UDV stack; pushes and pops happen inside the sweeps.
+class SvdStack {
+ public:
+  using Matrix = std::vector<double>;  // column-major N x N
+  using Vector = std::vector<double>;
+  SvdStack(const Model::HubbardAttractiveU& model, int side) : model_(&model), side_(side) {}
+  int MatDim() const { return model_->params().nl * model_->params().nl; }
+  int StackLength() const {
+    int n = 0;
+    check(hq_get_stack(model_->context(), 0, side_, &n, nullptr, nullptr, nullptr));
+    return n;
+  }
+  bool empty() const { return StackLength() == 0; }
+  Vector SingularValues() const { Vector d(MatDim()); get(nullptr, d.data(), nullptr); return d; }
+  Matrix MatrixU() const { Matrix u(size_t(MatDim()) * MatDim()); get(u.data(), nullptr, nullptr); return u; }
+  Matrix MatrixV() const { Matrix v(size_t(MatDim()) * MatDim()); get(nullptr, nullptr, v.data()); return v; }
+
+ private:
+  void get(double* u, double* d, double* v) const {
+    int n = 0;
+    check(hq_get_stack(model_->context(), 0, side_, &n, u, d, v));
+    if (n == 0) throw std::runtime_error("Utils::SvdStack: the stack is empty");
+  }
+  const Model::HubbardAttractiveU* model_;
+  int side_;
+};
+
+}  // namespace Utils
 
 namespace DQMC {
 

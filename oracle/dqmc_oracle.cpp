@@ -826,6 +826,22 @@ int or_run_schedule(void* h, int sweeps_warmup, int bin_num, int bin_capacity, i
   } catch (...) { return -1; }
 }
 
+// top of the left (side 0) or right (side 1) SVD stack as the product U S V^T of all its
+// entries (include/utils/svd_stack.hpp:83-103), column-major N x N; returns the stack length
+// (checker for hq_get_stack)
+int or_stack_top(void* h, int side, double* prod) {
+  auto* c = static_cast<Chain*>(h);
+  const SvdStack& st = side == 0 ? c->core.left : c->core.right;
+  if (st.empty()) return 0;
+  Mat us = st.U();
+  const Vec& sv = st.S();
+  for (int j = 0; j < us.n; ++j)
+    for (int i = 0; i < us.n; ++i) us(i, j) *= sv[j];
+  const Mat pr = gemm(us, false, st.V(), true);
+  std::copy(pr.a.begin(), pr.a.end(), prod);
+  return st.len;
+}
+
 // -------------------------------------------------------------------------------------
 //  log|det(1 + B_nt ... B_1)| of the current fields and its exact gradient identities
 //  (no counterpart in the reference; checker for the adjoint kernel).

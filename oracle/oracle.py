@@ -56,6 +56,8 @@ def lib():
         L.or_run_schedule.restype = i
         L.or_run_schedule.argtypes = [vp, i, i, i, i, i, i, ip, i, dp, dp, dp, dp]
         L.or_logdet.restype = d
+        L.or_stack_top.restype = i
+        L.or_stack_top.argtypes = [vp, i, dp]
         L.or_logdet.argtypes = [vp]
         L.or_logdet_grad.restype = i
         L.or_logdet_grad.argtypes = [vp, dp]
@@ -203,6 +205,12 @@ class OracleChain:
         if rc != 0:
             raise RuntimeError("or_run_schedule failed")
         return {"eq": eq[:bin_num], "spin": spin[:bin_num], "ldos": ldos[:bin_num], "gfk": gfk[:bin_num, : len(kl)]}
+
+    def stack_top(self, side):
+        """(length, U S V^T of the left (0) or right (1) SVD stack)."""
+        prod = np.zeros((self.ns, self.ns), order="F")
+        n = lib().or_stack_top(self.h, int(side), _dp(prod))
+        return n, prod
 
     def logdet(self):
         return lib().or_logdet(self.h)

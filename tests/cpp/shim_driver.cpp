@@ -29,5 +29,9 @@ int main(int argc, char** argv) {
   long s = 0;
   for (int v : f) s += v;
   std::printf("%ld\n", s);
+  // the stacks after an up + down pair: left empty, right holding every interval
+  Utils::SvdStack left(model, 0), right(model, 1);
+  const auto d = right.SingularValues();
+  std::printf("%d %d %d %.17g\n", left.StackLength(), right.StackLength(), right.MatDim(), d[0]);
   return 0;
 }

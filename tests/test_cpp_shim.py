@@ -39,3 +39,5 @@ def test_facade_driver_matches_oracle(tmp_path, oracle):
     assert abs(g00 - g[0, 0]) <= 1e-10 and abs(g11 - g[1, 1]) <= 1e-10
     assert fsum == int(o.fields().sum())
     assert 0.0 <= wrap < 1e-8
+    # Utils::SvdStack view: left empty, right holding the 4 intervals, positive scales
+    assert (int(out[4]), int(out[5]), int(out[6])) == (0, 4, 16) and float(out[7]) > 0.0

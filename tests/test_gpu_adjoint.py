@@ -125,3 +125,39 @@ def test_c4_batched_configurations(hq, oracle):
         g_b = -(grads[c][2][i, j] + grads[c][2][j, i])
         assert abs(g_b - fd_b) <= 1e-6 * max(1.0, abs(fd_b))
     e.close()
+
+
+def test_autograd_function_gradcheck(hq, oracle):
+    """The torch.autograd.Function wrapper: gradients with respect to the 2N bond hoppings,
+    mu and u against torch's own central differences of the GPU log-determinant."""
+    import torch
+    from hubbard_b200.autograd import LogDet
+
+    L, beta, nt, pace = 3, 1.0, 10, 5
+    N = L * L
+    H = nn_hop(L)
+    bonds = [(i, j) for i in range(N) for j in range(i + 1, N) if H[i, j] != 0]
+    fields = stream_fields(oracle, L, nt, 99, 1)[0]
+    rng = np.random.default_rng(5)
+    t = torch.tensor(1.0 + 0.1 * rng.standard_normal(len(bonds)), dtype=torch.float64, requires_grad=True)
+    mu = torch.tensor(-0.3, dtype=torch.float64, requires_grad=True)
+    u = torch.tensor(4.0, dtype=torch.float64, requires_grad=True)
+    ii = torch.tensor([b[0] for b in bonds])
+    jj = torch.tensor([b[1] for b in bonds])
+
+    def f(t_, mu_, u_):
+        hop = torch.zeros(N, N, dtype=torch.float64)
+        hop = hop.index_put((ii, jj), t_, accumulate=True).index_put((jj, ii), t_, accumulate=True)
+        return LogDet.apply(hop, mu_, u_, fields, beta, pace)
+
+    assert torch.autograd.gradcheck(f, (t, mu, u), eps=1e-5, atol=1e-5, rtol=1e-4)
+    # the value is the oracle's log-determinant of the same hopping matrix
+    hop = np.zeros((N, N))
+    tv = t.detach().numpy()
+    for k, (i, j) in enumerate(bonds):
+        hop[i, j] += tv[k]
+        hop[j, i] += tv[k]
+    o = oracle.OracleChain(L, u=4.0, mu=-0.3, beta=beta, nt=nt, pace=pace, seed=1, custom_hop=hop)
+    o.set_fields(fields)
+    ld = float(f(t, mu, u).detach())
+    assert abs(ld - o.logdet()) <= 1e-9 * max(1.0, abs(ld))

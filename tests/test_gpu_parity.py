@@ -237,3 +237,22 @@ def test_delay_depth_does_not_change_the_chain(hq, oracle, delay):
     assert np.abs(e.g(0) - o.g()).max() <= 1e-10
     assert e.config(0)[1] == delay
     e.close()
+
+
+def test_svd_stack_products_match_the_reference(hq, oracle):
+    """hq_get_stack (the Utils::SvdStack surface): the product U diag(D) V^T of the top of each
+    stack equals the reference's U S V^T of the same B products, at tau = 0 and at beta."""
+    e, o = pair(hq, oracle, seed=9)
+    for d, side_full in ((None, 1), (UP, 0), (DOWN, 1)):
+        if d is not None:
+            e.sweep(d)
+            o.sweep(d)
+        for side in (0, 1):
+            n, U, D, V = e.stack(0, side)
+            n_ref, prod_ref = o.stack_top(side)
+            assert n == n_ref == (4 if side == side_full else 0), (d, side, n, n_ref)
+            if n:
+                prod = (U * D) @ V.T
+                assert np.abs(U.T @ U - np.eye(16)).max() <= 1e-12
+                assert np.abs(prod - prod_ref).max() <= 1e-10 * np.abs(prod_ref).max()
+    e.close()
