@@ -358,11 +358,20 @@ struct ProfScope {
     }
     idx = c->prof_next++;
     c->prof[idx].cls = cls;
-    HQ_CUDA(cudaEventRecordWithFlags(c->prof[idx].e0, c->stream, cudaEventRecordExternal));
+    // inside a stream capture the records become graph nodes (external events); outside
+    // one they are plain records
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    HQ_CUDA(cudaStreamIsCapturing(c->stream, &cs));
+    capturing = cs == cudaStreamCaptureStatusActive;
+    if (capturing) HQ_CUDA(cudaEventRecordWithFlags(c->prof[idx].e0, c->stream, cudaEventRecordExternal));
+    else HQ_CUDA(cudaEventRecord(c->prof[idx].e0, c->stream));
   }
   ~ProfScope() {
-    if (idx != size_t(-1)) cudaEventRecordWithFlags(c->prof[idx].e1, c->stream, cudaEventRecordExternal);
+    if (idx == size_t(-1)) return;
+    if (capturing) cudaEventRecordWithFlags(c->prof[idx].e1, c->stream, cudaEventRecordExternal);
+    else cudaEventRecord(c->prof[idx].e1, c->stream);
   }
+  bool capturing = false;
 };
 
 void run_jobs(hq_ctx* c, int phase, int dir, int b) {

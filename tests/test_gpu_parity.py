@@ -256,3 +256,41 @@ def test_svd_stack_products_match_the_reference(hq, oracle):
                 assert np.abs(U.T @ U - np.eye(16)).max() <= 1e-12
                 assert np.abs(prod - prod_ref).max() <= 1e-10 * np.abs(prod_ref).max()
     e.close()
+
+
+def test_c5_lattice_on_the_non_resident_path(hq, oracle):
+    """16x16 (N = 256, the C5 lattice): G no longer fits in one SM's shared memory, so every
+    kernel runs on its global-memory path. Shortened to beta = 0.8 (16 slices, pace 8)."""
+    e, o = pair(hq, oracle, L=16, mu=-0.2, beta=0.8, nt=16, pace=8, seed=5000, snapshots=0)
+    assert np.array_equal(e.fields(0), o.fields())
+    g = o.g()
+    assert np.abs(e.g(0) - g).max() <= 1e-10 * max(1.0, np.abs(g).max())
+    for d in (UP, DOWN):
+        e.sweep(d, hq.SWEEP_MEASURE)
+        o.sweep(d)
+        assert np.array_equal(e.fields(0), o.fields())
+        g = o.g()
+        floor = max(1e-10, 10 * o.wrap_errors()[0])
+        assert np.abs(e.g(0) - g).max() <= floor * max(1.0, np.abs(g).max())
+    est = e.estimators(0)
+    assert est[4] == 2 * 16 * 256 and est[5] == o.counts()[1]
+    e.close()
+
+
+def test_profiling_with_and_without_graphs(hq):
+    """Per-launch device times (hq_profile_collect) of a plain sweep and of a graph replay."""
+    e = hq.Engine([dict(nl=4, u=4.0, beta=4.0, nt=40, stabilization_pace=10, seed=2)])
+    e.fields_random()
+    e.init()
+    e.profile_enable(True)
+    classes = hq.capi.PROFILE_CLASSES
+    for use_graph, d in ((False, UP), (True, DOWN)):
+        if use_graph:
+            e.capture_graph(d, hq.SWEEP_MEASURE)
+        ms = np.zeros(len(classes))
+        cnt = np.zeros(len(classes), dtype=np.int64)
+        e.sweep(d, hq.SWEEP_MEASURE)
+        e.profile_collect(ms, cnt)
+        i = classes.index("interval")
+        assert cnt[i] == 4 and ms[i] > 0.0, (use_graph, cnt, ms)
+    e.close()
