@@ -26,7 +26,7 @@ EXPORTS = [
     "hq_get_wrap_errors", "hq_get_estimators", "hq_get_dynamic_estimators", "hq_reset_estimators",
     "hq_ratio_log", "hq_logdet_adjoint", "hq_capture_graph", "hq_launch_graph", "hq_get_config",
     "hq_upload_fields_i8", "hq_download_fields_i8", "hq_get_stream", "hq_profile_enable", "hq_profile_collect",
-    "hq_equaltime_g_noalloc", "hq_autotune", "hq_get_stack",
+    "hq_equaltime_g_noalloc", "hq_autotune", "hq_get_stack", "hq_get_rng_state", "hq_set_rng_state",
 ]
 PROFILE_CLASSES = ["interval", "bchain", "udt", "gemm", "invert", "measure", "dynamic", "adjoint"]
 
@@ -106,6 +106,8 @@ def lib():
             "hq_equaltime_g_noalloc": [c_int, c_dbl, c_dbl, c_dbl, c_dbl, c_int, c_int, vp, vp, vp],
             "hq_autotune": [vp, c_int, ctypes.POINTER(HqTuneEntry), c_int, ip],
             "hq_get_stack": [vp, c_int, c_int, ip, dp, dp, dp],
+            "hq_get_rng_state": [vp, c_int, ctypes.POINTER(ctypes.c_uint)],
+            "hq_set_rng_state": [vp, c_int, ctypes.c_uint],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -276,6 +278,14 @@ class Engine:
         U, V, D = np.zeros((N, N), order="F"), np.zeros((N, N), order="F"), np.zeros(N)
         check(lib().hq_get_stack(self.h, chain, side, ctypes.byref(n), _dp(U), _dp(D), _dp(V)))
         return n.value, U, D, V
+
+    def rng_state(self, chain):
+        v = ctypes.c_uint(0)
+        check(lib().hq_get_rng_state(self.h, chain, ctypes.byref(v)))
+        return v.value
+
+    def set_rng_state(self, chain, state):
+        check(lib().hq_set_rng_state(self.h, chain, int(state)))
 
     def stream(self):
         s = ctypes.c_void_p()

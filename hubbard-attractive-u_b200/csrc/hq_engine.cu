@@ -749,6 +749,31 @@ int hq_get_fields(hq_ctx* c, int chain, int* fields) {
   HQ_API_END
 }
 
+// State word of a chain's minstd_rand0 engine (the reference's Utils::Random engine,
+// src/random.cpp:14-15): saved with the fields it makes a checkpoint from which the chain
+// continues exactly (fields, then this word, then hq_init_stacks_and_g).
+int hq_get_rng_state(hq_ctx* c, int chain, unsigned int* state) {
+  HQ_API_BEGIN
+  check_chain(c, chain);
+  if (!state) throw HqError(HQ_E_INVALID, "null state");
+  uint32_t v = 0;
+  HQ_CUDA(cudaMemcpyAsync(&v, c->desc[chain].rng, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  HQ_CUDA(cudaStreamSynchronize(c->stream));
+  *state = v;
+  HQ_API_END
+}
+
+int hq_set_rng_state(hq_ctx* c, int chain, unsigned int state) {
+  HQ_API_BEGIN
+  check_chain(c, chain);
+  if (state == 0u || state >= 2147483647u) throw HqError(HQ_E_RANGE, "minstd_rand0 state must be in [1, 2147483646]");
+  uint32_t v = state;
+  HQ_CUDA(cudaMemcpyAsync(c->desc[chain].rng, &v, sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+  HQ_CUDA(cudaStreamSynchronize(c->stream));
+  c->ch[chain].rng_after_fields = v;
+  HQ_API_END
+}
+
 int hq_init_stacks_and_g(hq_ctx* c) {
   HQ_API_BEGIN
   if (!c) throw HqError(HQ_E_INVALID, "null context");

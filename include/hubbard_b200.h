@@ -175,6 +175,13 @@ HQ_API int hq_get_config(hq_ctx* ctx, int chain, int* expk_mode, int* delay_dept
  * Between sweeps the stacks are at tau = 0 (left empty) or at tau = beta (right empty). */
 HQ_API int hq_get_stack(hq_ctx* ctx, int chain, int side, int* length, double* U, double* D, double* V);
 
+/* State word of a chain's minstd_rand0 engine (Utils::Random, src/random.cpp:14-15). With the
+ * fields (hq_get_fields / hq_set_fields) it is a checkpoint: after hq_set_fields,
+ * hq_set_rng_state and hq_init_stacks_and_g the chain continues exactly as it would have from
+ * tau = 0. The state must lie in [1, 2147483646]. */
+HQ_API int hq_get_rng_state(hq_ctx* ctx, int chain, unsigned int* state);
+HQ_API int hq_set_rng_state(hq_ctx* ctx, int chain, unsigned int state);
+
 /* One timed candidate of hq_autotune. */
 typedef struct {
   int nl;              /* lattice size of the group of chains */

@@ -6,6 +6,8 @@ ising.fields) and writes:
   example_run.json     : observables (mean, stddev, stderr, per-bin values), wrap errors
   example_fields.txt   : the final field configuration, "nt ns" then nt rows of ns +-1
   example_config.toml  : the run's configuration file (verbatim)
+  example_format.json  : verbatim lines of momenta.out, tgrids.out, ising.fields and of the
+                         binned output files (format checks of the result writers)
 Usage: python tests/golden/make_golden.py /path/to/reference
 """
 import json
@@ -61,7 +63,16 @@ def main(ref):
             g.write(" ".join("%d" % v for v in row) + "\n")
     with open(os.path.join(ex, "config.toml")) as src, open(os.path.join(HERE, "example_config.toml"), "w") as dst:
         dst.write(src.read())
-    print("wrote example_run.json, example_fields.txt, example_config.toml")
+    # verbatim lines of the output files, for the writers' format checks
+    fmt = {}
+    for name, nlines in (("momenta.out", None), ("tgrids.out", None), ("ising.fields", 6), ("filling.bins.out", 5),
+                         ("gf.bins.out", 5), ("spin_corr.bins.out", 5), ("gf.out", 3)):
+        lines = open(os.path.join(ex, name)).read().split("\n")
+        lines = [ln for ln in lines if ln.strip()]
+        fmt[name] = lines if nlines is None else lines[:nlines]
+    with open(os.path.join(HERE, "example_format.json"), "w") as f:
+        json.dump(fmt, f, indent=0)
+    print("wrote example_run.json, example_fields.txt, example_config.toml, example_format.json")
 
 
 if __name__ == "__main__":
