@@ -173,6 +173,15 @@ struct hq_ctx {
   struct ProfEv { int cls; cudaEvent_t e0, e1; };
   std::vector<ProfEv> prof;
   size_t prof_next = 0;
+  // chain groups of the up / down sweeps: each group's kernels run on its own stream, so that
+  // one group's launches fill the SMs left idle by the other's last wave
+  static constexpr int kGroups = 2;
+  int ngroups = 1;
+  cudaStream_t gstream[kGroups] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[kGroups] = {nullptr, nullptr};
+  // the chains and stream the launch helpers currently issue for (default: all, main stream)
+  int cur_c0 = 0, cur_n = 0;
+  cudaStream_t cur_st = nullptr;
   bool at_zero = false;         // stacks at tau = 0 (left empty, right full)
   bool at_beta = false;         // stacks at tau = beta
   bool initialised = false;
@@ -184,6 +193,11 @@ struct hq_ctx {
     if (arena) cudaFree(arena);
     for (auto* p : extra_allocs) cudaFree(p);
     for (auto& e : prof) { cudaEventDestroy(e.e0); cudaEventDestroy(e.e1); }
+    for (int g = 0; g < kGroups; ++g) {
+      if (gstream[g] && gstream[g] != stream) cudaStreamDestroy(gstream[g]);
+      if (ev_join[g]) cudaEventDestroy(ev_join[g]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -360,25 +374,44 @@ struct ProfScope {
     c->prof[idx].cls = cls;
     // inside a stream capture the records become graph nodes (external events); outside
     // one they are plain records
+    st = c->cur_st ? c->cur_st : c->stream;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    HQ_CUDA(cudaStreamIsCapturing(c->stream, &cs));
+    HQ_CUDA(cudaStreamIsCapturing(st, &cs));
     capturing = cs == cudaStreamCaptureStatusActive;
-    if (capturing) HQ_CUDA(cudaEventRecordWithFlags(c->prof[idx].e0, c->stream, cudaEventRecordExternal));
-    else HQ_CUDA(cudaEventRecord(c->prof[idx].e0, c->stream));
+    if (capturing) HQ_CUDA(cudaEventRecordWithFlags(c->prof[idx].e0, st, cudaEventRecordExternal));
+    else HQ_CUDA(cudaEventRecord(c->prof[idx].e0, st));
   }
   ~ProfScope() {
     if (idx == size_t(-1)) return;
-    if (capturing) cudaEventRecordWithFlags(c->prof[idx].e1, c->stream, cudaEventRecordExternal);
-    else cudaEventRecord(c->prof[idx].e1, c->stream);
+    if (capturing) cudaEventRecordWithFlags(c->prof[idx].e1, st, cudaEventRecordExternal);
+    else cudaEventRecord(c->prof[idx].e1, st);
   }
+  cudaStream_t st = nullptr;
   bool capturing = false;
 };
+
+// the launch range of the current chain group
+struct Cur {
+  const HqChain* d;
+  int n;
+  cudaStream_t st;
+};
+Cur cur(hq_ctx* c) {
+  if (!c->cur_st) return {c->d_desc, c->n, c->stream};
+  return {c->d_desc + c->cur_c0, c->cur_n, c->cur_st};
+}
 
 void run_jobs(hq_ctx* c, int phase, int dir, int b) {
   ProfScope ps(c, PC_GEMM);
   auto it = c->jobs.find(std::make_tuple(phase, dir, b));
   if (it == c->jobs.end()) throw HqError(HQ_E_INVALID, "internal: missing job list");
-  HQ_CUDA(hq::launch_gemm(it->second.first, it->second.second, c->Nmax, c->Nmax, c->stream));
+  if (c->cur_st) {
+    // per-chain phases hold one job per chain, in chain order
+    if (it->second.second != c->n) throw HqError(HQ_E_INVALID, "internal: job list is not per chain");
+    HQ_CUDA(hq::launch_gemm(it->second.first + c->cur_c0, c->cur_n, c->Nmax, c->Nmax, c->cur_st));
+  } else {
+    HQ_CUDA(hq::launch_gemm(it->second.first, it->second.second, c->Nmax, c->Nmax, c->stream));
+  }
 }
 
 void upload_desc(hq_ctx* c) {
@@ -388,16 +421,18 @@ void upload_desc(hq_ctx* c) {
 
 // one stack push of interval b: bchain -> UDV -> cumulative Vt
 void push_step(hq_ctx* c, int dir_kernel, int dir_jobs, int b) {
-  { ProfScope ps(c, PC_BCHAIN); HQ_CUDA(hq::launch_bchain(c->d_desc, c->n, dir_kernel, b, c->Nmax, c->resident, c->stream)); }
+  const Cur g = cur(c);
+  { ProfScope ps(c, PC_BCHAIN); HQ_CUDA(hq::launch_bchain(g.d, g.n, dir_kernel, b, c->Nmax, c->resident, g.st)); }
   const int side = (dir_kernel == HQ_DOWN) ? 1 : 0;
-  { ProfScope ps(c, PC_UDT); HQ_CUDA(hq::launch_udt(c->d_desc, c->n, side, b, c->Nmax, c->resident, c->stream)); }
+  { ProfScope ps(c, PC_UDT); HQ_CUDA(hq::launch_udt(g.d, g.n, side, b, c->Nmax, c->resident, g.st)); }
   run_jobs(c, PH_PUSH, dir_jobs, b);
 }
 
 void builder_equaltime(hq_ctx* c, int dir_jobs, int b) {
+  const Cur g = cur(c);
   run_jobs(c, PH_B1, dir_jobs, b);
   run_jobs(c, PH_B2, dir_jobs, b);
-  { ProfScope ps(c, PC_INVERT); HQ_CUDA(hq::launch_invert(c->d_desc, c->n, b, 0, c->Nmax, c->resident, c->stream)); }
+  { ProfScope ps(c, PC_INVERT); HQ_CUDA(hq::launch_invert(g.d, g.n, b, 0, c->Nmax, c->resident, g.st)); }
   run_jobs(c, PH_B3, dir_jobs, b);
   run_jobs(c, PH_B4, dir_jobs, b);
 }
@@ -406,11 +441,32 @@ void issue_sweep(hq_ctx* c, int dir, int flags) {
   c->prof_next = 0;
   const int kf = flags & (HQ_F_MEASURE | HQ_F_SNAPSHOT | HQ_F_LOG_RATIOS);
   if (dir == HQ_UP || dir == HQ_DOWN) {
-    for (int b = 0; b < c->nstab_max; ++b) {
-      { ProfScope ps(c, PC_INTERVAL); HQ_CUDA(hq::launch_interval(c->d_desc, c->n, dir, b, kf, c->Nmax, c->kmax_max, c->resident, c->stream)); }
-      push_step(c, dir, dir, b);
-      builder_equaltime(c, dir, b);
-      if (kf & (HQ_F_MEASURE | HQ_F_SNAPSHOT)) { ProfScope ps(c, PC_MEASURE); HQ_CUDA(hq::launch_measure(c->d_desc, c->n, dir, b, kf, c->stream)); }
+    // the chain groups fork from the main stream, run concurrently, and join it again
+    const int G = c->ngroups;
+    if (G > 1) {
+      HQ_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+      for (int g = 1; g < G; ++g) HQ_CUDA(cudaStreamWaitEvent(c->gstream[g], c->ev_fork, 0));
+    }
+    for (int g = 0; g < G; ++g) {
+      if (G > 1) {
+        c->cur_c0 = (c->n * g) / G;
+        c->cur_n = (c->n * (g + 1)) / G - c->cur_c0;
+        c->cur_st = c->gstream[g];
+      }
+      const Cur gr = cur(c);
+      for (int b = 0; b < c->nstab_max; ++b) {
+        { ProfScope ps(c, PC_INTERVAL); HQ_CUDA(hq::launch_interval(gr.d, gr.n, dir, b, kf, c->Nmax, c->kmax_max, c->resident, gr.st)); }
+        push_step(c, dir, dir, b);
+        builder_equaltime(c, dir, b);
+        if (kf & (HQ_F_MEASURE | HQ_F_SNAPSHOT)) { ProfScope ps(c, PC_MEASURE); HQ_CUDA(hq::launch_measure(gr.d, gr.n, dir, b, kf, gr.st)); }
+      }
+    }
+    c->cur_st = nullptr;
+    if (G > 1) {
+      for (int g = 1; g < G; ++g) {
+        HQ_CUDA(cudaEventRecord(c->ev_join[g], c->gstream[g]));
+        HQ_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join[g], 0));
+      }
     }
   } else {
     { ProfScope ps(c, PC_DYN); HQ_CUDA(hq::launch_dyn_start(c->d_desc, c->n, c->stream)); }
@@ -471,6 +527,13 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   c->device = device;
   HQ_CUDA(cudaSetDevice(device));
   HQ_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  if (n_chains >= 32) {
+    c->ngroups = hq_ctx::kGroups;
+    c->gstream[0] = c->stream;
+    for (int g = 1; g < c->ngroups; ++g) HQ_CUDA(cudaStreamCreateWithFlags(&c->gstream[g], cudaStreamNonBlocking));
+    HQ_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    for (int g = 0; g < c->ngroups; ++g) HQ_CUDA(cudaEventCreateWithFlags(&c->ev_join[g], cudaEventDisableTiming));
+  }
   c->n = n_chains;
   c->ch.resize(n_chains);
   c->desc.resize(n_chains);
