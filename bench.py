@@ -314,8 +314,7 @@ def run_gpu(args):
         eng.init()                                     # stacks + G from the fields
         eng.sweep(hq.SWEEP_UP, hq.SWEEP_MEASURE)
         eng.download_fields_i8(host_fields.data_ptr())  # d2h: updated fields
-        for c in range(n):
-            host_est[c] = eng.estimators(c)             # d2h: estimator sums (synchronises)
+        host_est = eng.estimators_all()                 # d2h: every chain's estimator sums (synchronises)
     eng.sync()
     e2e_s = time.perf_counter() - t0
     if dist:
@@ -376,7 +375,7 @@ def run_gpu(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": ({"value": e2e_value, "unit": "sweeps/s", "h2d_bytes_per_step": nbytes,
-                     "d2h_bytes_per_step": nbytes + n * 6 * 8,
+                     "d2h_bytes_per_step": nbytes + n * 16 * 8,
                      "step": "h2d fields -> hq_init_stacks_and_g -> hq_sweep(up) -> d2h fields + estimators"}
                     if e2e_value else None),
             "gpu_launches": gpu_launches,

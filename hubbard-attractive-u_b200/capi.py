@@ -23,7 +23,7 @@ EXPK_DENSE, EXPK_SEPARABLE, EXPK_AUTO = 0, 1, -1
 EXPORTS = [
     "hq_last_error", "hq_create", "hq_destroy", "hq_set_hopping", "hq_fields_random", "hq_set_fields",
     "hq_get_fields", "hq_init_stacks_and_g", "hq_sweep", "hq_sync", "hq_get_g", "hq_set_g",
-    "hq_get_wrap_errors", "hq_get_estimators", "hq_get_dynamic_estimators", "hq_reset_estimators",
+    "hq_get_wrap_errors", "hq_get_estimators", "hq_get_estimators_all", "hq_get_dynamic_estimators", "hq_reset_estimators",
     "hq_ratio_log", "hq_logdet_adjoint", "hq_capture_graph", "hq_launch_graph", "hq_get_config",
     "hq_upload_fields_i8", "hq_download_fields_i8", "hq_get_stream", "hq_profile_enable", "hq_profile_collect",
     "hq_equaltime_g_noalloc", "hq_autotune", "hq_get_stack", "hq_get_rng_state", "hq_set_rng_state",
@@ -91,6 +91,7 @@ def lib():
             "hq_set_g": [vp, c_int, dp],
             "hq_get_wrap_errors": [vp, c_int, dp],
             "hq_get_estimators": [vp, c_int, dp],
+            "hq_get_estimators_all": [vp, dp],
             "hq_get_dynamic_estimators": [vp, c_int, dp, dp, dp],
             "hq_reset_estimators": [vp, c_int],
             "hq_ratio_log": [vp, c_int, c_ll, dp, c_ll, ctypes.POINTER(c_ll)],
@@ -214,6 +215,12 @@ class Engine:
     def estimators(self, chain):
         out = np.zeros(6)
         check(lib().hq_get_estimators(self.h, chain, _dp(out)))
+        return out
+
+    def estimators_all(self):
+        """The six estimator sums of every chain as an (n_chains, 6) array, one copy."""
+        out = np.zeros((self.n, 6))
+        check(lib().hq_get_estimators_all(self.h, _dp(out)))
         return out
 
     def dynamic_estimators(self, chain):

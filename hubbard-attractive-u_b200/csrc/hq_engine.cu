@@ -154,6 +154,9 @@ struct hq_ctx {
   std::vector<ChainHost> ch;
   std::vector<HqChain> desc;
   HqChain* d_desc = nullptr;
+  // every chain's accumulators gathered chain-major (device) and its pinned host copy
+  double* d_acc_all = nullptr;
+  double* h_acc_all = nullptr;
   char* arena = nullptr;
   size_t arena_bytes = 0;
   std::vector<void*> extra_allocs;
@@ -190,6 +193,8 @@ struct hq_ctx {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
     if (d_jobs) cudaFree(d_jobs);
     if (d_desc) cudaFree(d_desc);
+    if (d_acc_all) cudaFree(d_acc_all);
+    if (h_acc_all) cudaFreeHost(h_acc_all);
     if (arena) cudaFree(arena);
     for (auto* p : extra_allocs) cudaFree(p);
     for (auto& e : prof) { cudaEventDestroy(e.e0); cudaEventDestroy(e.e1); }
@@ -437,22 +442,38 @@ void builder_equaltime(hq_ctx* c, int dir_jobs, int b) {
   run_jobs(c, PH_B4, dir_jobs, b);
 }
 
+// Runs body() once per chain group, each group on its own stream forked from the main
+// stream, and joins the groups back into the main stream. One group's launches fill the
+// SMs that the other's last wave leaves idle. With one group body() runs on the main stream.
+template <class F>
+void in_groups(hq_ctx* c, F&& body) {
+  const int G = c->ngroups;
+  if (G > 1) {
+    HQ_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+    for (int g = 1; g < G; ++g) HQ_CUDA(cudaStreamWaitEvent(c->gstream[g], c->ev_fork, 0));
+  }
+  for (int g = 0; g < G; ++g) {
+    if (G > 1) {
+      c->cur_c0 = (c->n * g) / G;
+      c->cur_n = (c->n * (g + 1)) / G - c->cur_c0;
+      c->cur_st = c->gstream[g];
+    }
+    body();
+  }
+  c->cur_st = nullptr;
+  if (G > 1) {
+    for (int g = 1; g < G; ++g) {
+      HQ_CUDA(cudaEventRecord(c->ev_join[g], c->gstream[g]));
+      HQ_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join[g], 0));
+    }
+  }
+}
+
 void issue_sweep(hq_ctx* c, int dir, int flags) {
   c->prof_next = 0;
   const int kf = flags & (HQ_F_MEASURE | HQ_F_SNAPSHOT | HQ_F_LOG_RATIOS);
   if (dir == HQ_UP || dir == HQ_DOWN) {
-    // the chain groups fork from the main stream, run concurrently, and join it again
-    const int G = c->ngroups;
-    if (G > 1) {
-      HQ_CUDA(cudaEventRecord(c->ev_fork, c->stream));
-      for (int g = 1; g < G; ++g) HQ_CUDA(cudaStreamWaitEvent(c->gstream[g], c->ev_fork, 0));
-    }
-    for (int g = 0; g < G; ++g) {
-      if (G > 1) {
-        c->cur_c0 = (c->n * g) / G;
-        c->cur_n = (c->n * (g + 1)) / G - c->cur_c0;
-        c->cur_st = c->gstream[g];
-      }
+    in_groups(c, [&] {
       const Cur gr = cur(c);
       for (int b = 0; b < c->nstab_max; ++b) {
         { ProfScope ps(c, PC_INTERVAL); HQ_CUDA(hq::launch_interval(gr.d, gr.n, dir, b, kf, c->Nmax, c->kmax_max, c->resident, gr.st)); }
@@ -460,14 +481,7 @@ void issue_sweep(hq_ctx* c, int dir, int flags) {
         builder_equaltime(c, dir, b);
         if (kf & (HQ_F_MEASURE | HQ_F_SNAPSHOT)) { ProfScope ps(c, PC_MEASURE); HQ_CUDA(hq::launch_measure(gr.d, gr.n, dir, b, kf, gr.st)); }
       }
-    }
-    c->cur_st = nullptr;
-    if (G > 1) {
-      for (int g = 1; g < G; ++g) {
-        HQ_CUDA(cudaEventRecord(c->ev_join[g], c->gstream[g]));
-        HQ_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join[g], 0));
-      }
-    }
+    });
   } else {
     { ProfScope ps(c, PC_DYN); HQ_CUDA(hq::launch_dyn_start(c->d_desc, c->n, c->stream)); }
     for (int b = 0; b < c->nstab_max; ++b) {
@@ -843,20 +857,19 @@ int hq_init_stacks_and_g(hq_ctx* c) {
   for (auto& h : c->ch)
     if (!h.fields_set) throw HqError(HQ_E_INVALID, "fields of a chain are not set (hq_fields_random / hq_set_fields)");
   c->prof_next = 0;
-  // src/dqmc_core.cpp:67-87: right stack from t = nt down to 1 with B^T, push every pace
-  for (int b = 0; b < c->nstab_max; ++b) push_step(c, HQ_DOWN, 2, b);
-  // src/dqmc_core.cpp:89-97: G(0,0) from (empty left, full right)
-  const int last = c->nstab_max;  // job lists of dir 2 at b give right top b: use each chain's own top
-  (void)last;
   // builder with each chain's full right stack: the dir-2 job list at b = n_stab-1 of each chain.
   // Chains of different n_stab need their own b; issue one launch per distinct n_stab.
   std::vector<int> nstabs;
   for (auto& h : c->ch) nstabs.push_back(h.n_stab);
   std::sort(nstabs.begin(), nstabs.end());
   nstabs.erase(std::unique(nstabs.begin(), nstabs.end()), nstabs.end());
-  if (nstabs.size() == 1) {
-    builder_equaltime(c, 2, nstabs[0] - 1);
-  } else {
+  in_groups(c, [&] {
+    // src/dqmc_core.cpp:67-87: right stack from t = nt down to 1 with B^T, push every pace
+    for (int b = 0; b < c->nstab_max; ++b) push_step(c, HQ_DOWN, 2, b);
+    // src/dqmc_core.cpp:89-97: G(0,0) from (empty left, full right)
+    if (nstabs.size() == 1) builder_equaltime(c, 2, nstabs[0] - 1);
+  });
+  if (nstabs.size() > 1) {
     for (int ns : nstabs) {
       // deactivate chains with other stack lengths for this pass
       std::vector<HqChain> saved = c->desc;
@@ -1003,6 +1016,30 @@ int hq_get_estimators(hq_ctx* c, int chain, double* out6) {
   out6[3] = acc[HQ_ACC_NSLICE];
   out6[4] = acc[HQ_ACC_PROPOSED];
   out6[5] = acc[HQ_ACC_ACCEPTED];
+  HQ_API_END
+}
+
+int hq_get_estimators_all(hq_ctx* c, double* out) {
+  HQ_API_BEGIN
+  if (!c || !out) throw HqError(HQ_E_INVALID, "null argument");
+  const size_t cnt = size_t(c->n) * HQ_ACC_COUNT;
+  if (!c->d_acc_all) {
+    HQ_CUDA(cudaMalloc(&c->d_acc_all, cnt * sizeof(double)));
+    HQ_CUDA(cudaMallocHost(&c->h_acc_all, cnt * sizeof(double)));
+  }
+  HQ_CUDA(hq::launch_gather_acc(c->d_desc, c->n, c->d_acc_all, c->stream));
+  HQ_CUDA(cudaMemcpyAsync(c->h_acc_all, c->d_acc_all, cnt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  HQ_CUDA(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < c->n; ++i) {
+    const double* acc = c->h_acc_all + size_t(i) * HQ_ACC_COUNT;
+    double* o = out + size_t(i) * 6;
+    o[0] = acc[HQ_ACC_FILLING];
+    o[1] = acc[HQ_ACC_DOCC];
+    o[2] = acc[HQ_ACC_SWAVE];
+    o[3] = acc[HQ_ACC_NSLICE];
+    o[4] = acc[HQ_ACC_PROPOSED];
+    o[5] = acc[HQ_ACC_ACCEPTED];
+  }
   HQ_API_END
 }
 

@@ -1747,4 +1747,18 @@ cudaError_t launch_dyn_commit(const HqChain* chains, int n, int b, cudaStream_t 
   return cudaGetLastError();
 }
 
+// Copies every chain's accumulator block into one chain-major buffer, so that a single
+// device-to-host copy reads the estimators of all chains.
+__global__ void k_gather_acc(const HqChain* chains, int n, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * HQ_ACC_COUNT) return;
+  const int c = i / HQ_ACC_COUNT;
+  out[i] = chains[c].acc[i - c * HQ_ACC_COUNT];
+}
+cudaError_t launch_gather_acc(const HqChain* chains, int n, double* out, cudaStream_t st) {
+  const int total = n * HQ_ACC_COUNT;
+  k_gather_acc<<<(total + 255) / 256, 256, 0, st>>>(chains, n, out);
+  return cudaGetLastError();
+}
+
 }  // namespace hq

@@ -24,6 +24,7 @@ cudaError_t launch_dyn_slices(const HqChain* chains, int n, int b, int flags, in
 cudaError_t launch_dyn_measure(const HqChain* chains, int n, int b, int last_only, cudaStream_t st);
 cudaError_t launch_dyn_store(const HqChain* chains, int n, int b, cudaStream_t st);
 cudaError_t launch_dyn_commit(const HqChain* chains, int n, int b, cudaStream_t st);
+cudaError_t launch_gather_acc(const HqChain* chains, int n, double* out, cudaStream_t st);
 cudaError_t launch_adj_interval(const HqChain* chains, int n, int b, int Nmax, bool resident, cudaStream_t st);
 cudaError_t launch_adj_last(const HqChain* chains, int n, int b, cudaStream_t st);
 }  // namespace hq

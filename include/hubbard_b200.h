@@ -129,6 +129,10 @@ HQ_API int hq_get_wrap_errors(hq_ctx* ctx, int chain, double* out2);
  * out[3] number of measured slices, out[4] proposals, out[5] accepted flips.
  * (include/observable_methods.hpp:39-151; divide by out[3] for the per-slice mean.) */
 HQ_API int hq_get_estimators(hq_ctx* ctx, int chain, double* out6);
+/* The same six sums for every chain at once, chain-major: out[6*chain + k]. One gather
+ * launch and one device-to-host copy, instead of one copy per chain. (The reference runs
+ * one chain per process and reads its estimators in place.) */
+HQ_API int hq_get_estimators_all(hq_ctx* ctx, double* out);
 /* Displaced estimator sums: spin[nt], ldos[nt] and the displacement-summed
  * g(d, tau) = sum_i G(tau,0)[i+d, i] as gd[N][nt] (include/observable_methods.hpp:84-195);
  * G(k,tau) = (1/N) sum_d cos(k.r_d) g(d,tau). Any pointer may be NULL. */

@@ -193,6 +193,42 @@ def test_uneven_batch(hq, oracle):
     e.close()
 
 
+def test_uneven_batch_in_chain_groups(hq, oracle):
+    """34 chains of uneven L, beta and stack length: enough chains that the initialisation
+    and the sweeps run as two chain groups on forked streams. Every chain follows its own
+    oracle chain, and the one-copy estimator read equals the per-chain reads."""
+    cfgs = []
+    for c in range(34):
+        cfgs.append(dict(nl=[4, 6][c % 2], u=[2.0, 4.0, 6.0][c % 3], mu=[0.0, -0.3][c % 2],
+                         beta=[2.0, 4.0, 3.0][c % 3], nt=[20, 40, 30][c % 3], stabilization_pace=10,
+                         seed=2000 + c, expk_mode=-1))
+    e = hq.Engine(cfgs)
+    orcs = []
+    for c, p in enumerate(cfgs):
+        e.fields_random(c)
+        o = oracle.OracleChain(p["nl"], u=p["u"], mu=p["mu"], beta=p["beta"], nt=p["nt"], pace=10,
+                               seed=p["seed"])
+        o.fields_random()
+        o.init()
+        orcs.append(o)
+    e.init()
+    for c, o in enumerate(orcs):
+        assert np.abs(e.g(c) - o.g()).max() <= 1e-10, c
+    e.reset_estimators()
+    for d in (UP, DOWN):
+        e.sweep(d, hq.SWEEP_MEASURE)
+        for o in orcs:
+            o.sweep(d)
+    allest = e.estimators_all()
+    assert allest.shape == (34, 6)
+    for c, o in enumerate(orcs):
+        assert np.array_equal(e.fields(c), o.fields()), c
+        assert np.abs(e.g(c) - o.g()).max() <= 1e-10, c
+        assert np.array_equal(allest[c], e.estimators(c)), c
+        assert allest[c, 3] == 2 * cfgs[c]["nt"], c
+    e.close()
+
+
 def test_graph_replay_is_identical(hq, oracle):
     cfg = dict(nl=6, u=4.0, beta=4.0, nt=40, stabilization_pace=10, seed=5)
     a = hq.Engine([cfg, dict(cfg, seed=6)])
