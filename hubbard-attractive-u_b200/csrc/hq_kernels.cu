@@ -77,6 +77,27 @@ __device__ __forceinline__ void copy_mat(double* dst, int ldd, const double* src
   HQ_FOR_EACH_ELEM(N, i, j) dst[i + (size_t)j * ldd] = src[i + (size_t)j * lds];
 }
 
+// 8-byte asynchronous global -> shared copy; zero-fills (reads 0 bytes of `src`, which
+// the callers keep pointing at the operand's base) when `valid` is false
+__device__ __forceinline__ void cp_async_8(double* dst, const double* src, bool valid) {
+  const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  const int nbytes = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(src), "r"(nbytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND)); }
+
+// global -> shared copy of an N x N column-major matrix (shared ld `ldd`): every element is
+// an asynchronous copy, all issued before one wait, so that the copy costs about one memory
+// latency rather than one per loop trip. On return this thread's copies have landed; the
+// caller's barrier makes all of them visible.
+__device__ __forceinline__ void load_mat_async(double* dst, int ldd, const double* src, int lds, int N) {
+  HQ_FOR_EACH_ELEM(N, i, j) cp_async_8(dst + i + (size_t)j * ldd, src + i + (size_t)j * lds, true);
+  cp_async_commit();
+  cp_async_wait<0>();
+}
+
 // ---------------------------------------------------------------------------------
 //  Metropolis sweep over the N sites of one slice: submatrix (block-delayed) updates.
 //
@@ -485,7 +506,7 @@ k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int 
     G = p;
     ld = interval_ld(N);
     p += (size_t)N * ld;
-    copy_mat(G, ld, ch.G, N, N);
+    load_mat_async(G, ld, ch.G, N, N);
   } else {
     G = ch.G;
     ld = N;
@@ -585,7 +606,18 @@ k_bchain(const HqChain* __restrict__ chains, int nchains, int dir, int b, int re
   const size_t NN = (size_t)N * N;
   const double* U = top >= 0 ? ch.stackU + ((size_t)side * ch.n_stab + top) * NN : nullptr;
   const double* D = top >= 0 ? ch.stackD + ((size_t)side * ch.n_stab + top) * N : nullptr;
-  HQ_FOR_EACH_ELEM(N, i, j) X[i + (size_t)j * ld] = U ? U[i + (size_t)j * N] * D[j] : (i == j ? 1.0 : 0.0);
+  if (U && resident) {
+    // U and D land in shared memory by asynchronous copies (D in the stage area), then
+    // the columns are scaled in place
+    for (int j = threadIdx.x; j < N; j += blockDim.x) cp_async_8(stage + j, D + j, true);
+    load_mat_async(X, ld, U, N, N);
+    __syncthreads();
+    HQ_FOR_EACH_ELEM(N, i, j) X[i + (size_t)j * ld] *= stage[j];
+  } else if (U) {
+    HQ_FOR_EACH_ELEM(N, i, j) X[i + (size_t)j * ld] = U[i + (size_t)j * N] * D[j];
+  } else {
+    HQ_FOR_EACH_ELEM(N, i, j) X[i + (size_t)j * ld] = (i == j ? 1.0 : 0.0);
+  }
   __syncthreads();
   const int nsl = t_hi - t_lo + 1;
   for (int step = 0; step < nsl; ++step) {
@@ -891,7 +923,13 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
     order[rank] = j;
   }
   __syncthreads();
-  HQ_FOR_EACH_ELEM(N, i, j) A[i + (size_t)j * ld] = X[i + (size_t)order[j] * N];
+  if (resident) {
+    HQ_FOR_EACH_ELEM(N, i, j) cp_async_8(A + i + (size_t)j * ld, X + i + (size_t)order[j] * N, true);
+    cp_async_commit();
+    cp_async_wait<0>();
+  } else {
+    HQ_FOR_EACH_ELEM(N, i, j) A[i + (size_t)j * ld] = X[i + (size_t)order[j] * N];
+  }
   __syncthreads();
   // ---- blocked Householder QR ----
   for (int p0 = 0; p0 < N; p0 += kQB) {
@@ -1078,7 +1116,7 @@ k_invert(const HqChain* __restrict__ chains, int nchains, int b, int which, int 
   double* A;
   int ld;
   double* p = smem;
-  if (resident) { A = p; ld = smem_ld(N); p += (size_t)N * ld; copy_mat(A, ld, src, N, N); }
+  if (resident) { A = p; ld = smem_ld(N); p += (size_t)N * ld; load_mat_async(A, ld, src, N, N); }
   else { A = src; ld = N; }
   const int ldp = panel_ld(N);
   double* Wp = p; p += (size_t)ldp * kGJ;   // N x kGJ, column-major
@@ -1199,16 +1237,6 @@ __device__ __forceinline__ double vscale(const double* v, int mode, int i) {
   return fmin(x, 1.0);
 }
 
-// 8-byte asynchronous global -> shared copy; zero-fills (reads 0 bytes of `src`, which
-// the callers keep pointing at the operand's base) when `valid` is false
-__device__ __forceinline__ void cp_async_8(double* dst, const double* src, bool valid) {
-  const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  const int nbytes = valid ? 8 : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(src), "r"(nbytes));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int NPEND>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND)); }
 
 // ---------------------------------------------------------------------------------
 //  k_gemm: batched C = alpha op(A) diag(ks) op(B) (row / column scalings, beta, wrap-error
@@ -1387,7 +1415,7 @@ k_dyn_slices(const HqChain* __restrict__ chains, int nchains, int b, int flags, 
   double* M;
   int ld;
   double* p = smem;
-  if (resident) { M = p; ld = smem_ld(N); p += (size_t)N * ld; copy_mat(M, ld, src, N, N); }
+  if (resident) { M = p; ld = smem_ld(N); p += (size_t)N * ld; load_mat_async(M, ld, src, N, N); }
   else { M = src; ld = N; }
   double* stage = p;
   __syncthreads();
@@ -1582,7 +1610,7 @@ k_adj_interval(const HqChain* __restrict__ chains, int nchains, int b, int resid
   double* G;
   int ld;
   double* p = smem;
-  if (resident) { G = p; ld = smem_ld(N); p += (size_t)N * ld; copy_mat(G, ld, ch.G, N, N); }
+  if (resident) { G = p; ld = smem_ld(N); p += (size_t)N * ld; load_mat_async(G, ld, ch.G, N, N); }
   else { G = ch.G; ld = N; }
   double* stage = p;
   __syncthreads();
