@@ -276,9 +276,11 @@ def run_gpu(args):
     else:
         flops_per_launch = None
     achieved = (flops_per_launch / (avg_launch_ms * 1e-3) / 1e12) if flops_per_launch else None
-    # DRAM bytes of one k_interval launch: ncu capture of the 32-chain case (one wave; 5.56 MB read,
-    # 0 written), scaled by the chains of this launch (the traffic is per-chain state)
-    traffic = 5.556e6 * n / 32 if dom_name == "interval" else None
+    # DRAM bytes of one k_interval launch: ncu capture of a 16-chain launch (2.864 MB read, 0
+    # written), scaled by the chains of one launch here (the traffic is per-chain state; with
+    # two chain groups a launch covers half of the chains)
+    chains_per_launch = n * (CFG["nt"] // CFG["stabilization_pace"]) * args.steps / max(1, int(cnt_cls[dom]))
+    traffic = 2.864e6 * chains_per_launch / 16 if dom_name == "interval" else None
     # the whole sweep in the dense-GEMM flop convention (6N^3 per slice, 2N^2 per accepted flip,
     # 33N^3 per stabilisation), over the measured step time
     N = CFG["nl"] ** 2
@@ -287,7 +289,7 @@ def run_gpu(args):
     sweep_tf = f_sweep / (ms * 1e-3) / 1e12
     roofline = {"bound": "tensor", "kernel": f"k_{dom_name}", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_read+write of one k_interval launch at 32 chains, scaled by chains",
+                "traffic_source": "ncu dram__bytes_read+write of one k_interval launch of 16 chains, scaled by chains",
                 "sweep_dense_equivalent": {"tflops": sweep_tf, "frac": (sweep_tf / peak) if peak else None,
                                            "convention": "F = nt*6N^3 + 2N^2*accepted + n_stab*33N^3 per chain-sweep"},
                 "peak_source": "measured cuBLAS DGEMM 8192^3 FP64 on this GPU (FP64 has no entry in MEASURED_PEAKS.json)",
