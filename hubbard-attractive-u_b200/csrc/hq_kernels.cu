@@ -278,6 +278,94 @@ __device__ __forceinline__ void walk_block(const HqChain& ch, const double* G, i
   acc_count += (lane == 0) ? (double)a : 0.0;
 }
 
+// the walk of a 16-site block with g tiled 4 rows x 2 columns per lane: lane 8 rg + cg holds
+// g[4 rg + a][2 cg + b] (a < 4, b < 2). A step needs column s for the lane's four rows, row s
+// for its two columns and the diagonal entry: 7 shuffles instead of the 10 of an 8 x 1 tile.
+// Every entry is updated with the same expression as in walk_block, so the two walks agree
+// bitwise. Records: lanes with cg < 4 write X[J_(4 rg + cg), m], lanes with rg < 2 write
+// Y[m, J_(2 cg + rg)].
+__device__ __forceinline__ void walk_block16(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0,
+                                             int nb, bool log, int slot, double& acc_count) {
+  constexpr int NB = 16;
+  const int lane = threadIdx.x & 31;
+  const int rg = lane >> 3, cg = lane & 7;
+  double r[4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int row = 4 * rg + a, col = 2 * cg + b;
+      r[a][b] = (row < nb && col < nb) ? G[b0 + row + (size_t)(b0 + col) * ld] : 0.0;
+    }
+  double dls[NB], thr[NB];
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    dls[s] = s < nb ? sh.dl[b0 + s] : 0.0;
+    thr[s] = s < nb ? sh.u[b0 + s] * (1.0 + dls[s]) : 0.0;
+  }
+  double xk[NB], yk[NB], myg = 0.0, myr = 0.0;
+  unsigned mask = 0u;
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    xk[s] = 0.0;
+    yk[s] = 0.0;
+    if (s < nb) {
+      // g[s][s]; column s at the lane's rows (held by lane 8 rg + s/2, column slot s&1);
+      // row s at the lane's columns (held by lane 8 (s/4) + cg, row slot s&3)
+      const double dg = __shfl_sync(0xffffffffu, r[s & 3][s & 1], 8 * (s >> 2) + (s >> 1));
+      double colr[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) colr[a] = __shfl_sync(0xffffffffu, r[a][s & 1], 8 * rg + (s >> 1));
+      double rowv[2];
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        rowv[b] = __shfl_sync(0xffffffffu, r[s & 3][b], 8 * (s >> 2) + cg) - (2 * cg + b == s ? 1.0 : 0.0);
+      const double dl = dls[s];
+      const double av = 1.0 + (1.0 - dg) * dl;
+      const double gam = dl / av;
+      if (log && lane == s) myr = (av * av) / (1.0 + dl);
+      const bool acc = thr[s] < av * av;
+      const double ge = acc ? gam : 0.0;
+      // the record row of this lane is 4 rg + cg (cg < 4), its record column 2 cg + rg (rg < 2)
+      double xs = colr[0];
+      xs = (cg == 1) ? colr[1] : xs;
+      xs = (cg == 2) ? colr[2] : xs;
+      xs = (cg == 3) ? colr[3] : xs;
+      xk[s] = ge * xs;
+      yk[s] = (rg & 1) ? rowv[1] : rowv[0];
+      if (lane == s) myg = gam;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const double f = ge * colr[a];
+#pragma unroll
+        for (int b = 0; b < 2; ++b) r[a][b] = fma(f, rowv[b], r[a][b]);
+      }
+      mask |= acc ? (1u << s) : 0u;
+    }
+  }
+  const int a = __popc(mask);
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    if (mask & (1u << s)) {
+      const int m = __popc(mask & ((1u << s) - 1u));
+      if (cg < 4) sh.xt[(4 * rg + cg) * NB + m] = xk[s];
+      if (rg < 2) sh.yt[(2 * cg + rg) * NB + m] = yk[s];
+    }
+  }
+  if (lane < nb) {
+    const bool acc = (mask >> lane) & 1u;
+    if (acc) {
+      const int m = __popc(mask & ((1u << lane) - 1u));
+      sh.qj[m] = b0 + lane;
+      sh.qg[m] = myg;
+    }
+    sh.flip[b0 + lane] = acc ? 1 : 0;
+    if (log) sh.rr[b0 + lane] = myr;
+  }
+  if (lane == 0) sh.ired[slot] = a;
+  acc_count += (lane == 0) ? (double)a : 0.0;
+}
+
 // panels of the a flips of block [b0, b0 + NB): the two triangular recurrences, one row of X
 // and one column of Y per thread; the coefficients of flip m are contiguous in the records
 // (xt / yt at row j_m - b0) and are read in 16-byte pairs
@@ -404,7 +492,10 @@ __device__ __forceinline__ void metropolis_slice_blk(const HqChain& ch, double* 
   __syncthreads();
   double acc_count = 0.0;
   for (int b0 = 0, bi = 0; b0 < N; b0 += NB, ++bi) {
-    if (warp == 0) walk_block<NB>(ch, G, ld, sh, b0, min(NB, N - b0), log, bi & 1, acc_count);
+    if (warp == 0) {
+      if constexpr (NB == 16) walk_block16(ch, G, ld, sh, b0, min(NB, N - b0), log, bi & 1, acc_count);
+      else walk_block<NB>(ch, G, ld, sh, b0, min(NB, N - b0), log, bi & 1, acc_count);
+    }
     __syncthreads();
     // the count alternates between two words: with no flush (a == 0) no barrier follows,
     // and warp 0 writes the next block's count while other warps may still read this one
