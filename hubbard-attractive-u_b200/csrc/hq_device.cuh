@@ -21,15 +21,20 @@ namespace hq {
 constexpr uint32_t kMinstdA = 16807u;
 constexpr uint32_t kMinstdM = 2147483647u;
 
+// a * x mod m for a, x < m = 2^31 - 1, exactly, without a division: with t = a x =
+// hi 2^31 + lo and 2^31 = 1 (mod m), t = lo + hi (mod m); two folds leave a value <= m + 1
 __host__ __device__ inline uint32_t minstd_mulmod(uint64_t a, uint64_t x) {
-  return static_cast<uint32_t>((a * x) % kMinstdM);
+  const uint64_t t = a * x;
+  uint64_t r = (t & kMinstdM) + (t >> 31);
+  r = (r & kMinstdM) + (r >> 31);
+  return static_cast<uint32_t>(r >= kMinstdM ? r - kMinstdM : r);
 }
 // a^k mod m
 __host__ __device__ inline uint32_t minstd_pow(uint64_t k) {
   uint64_t result = 1, base = kMinstdA;
   while (k) {
-    if (k & 1) result = (result * base) % kMinstdM;
-    base = (base * base) % kMinstdM;
+    if (k & 1) result = minstd_mulmod(result, base);
+    base = minstd_mulmod(base, base);
     k >>= 1;
   }
   return static_cast<uint32_t>(result);

@@ -45,7 +45,7 @@ __host__ __device__ inline size_t interval_smem_doubles(int N, int kmax, bool re
   const size_t panels = (size_t)panel_ld(N) * kmax * 2;
   const size_t stage = (size_t)8 * (((N + 15) & ~15) + 4);
   const size_t work = panels > stage ? panels : stage;
-  return mat + work + 3 * (size_t)N + (size_t)(N + 7) / 4 + 64;
+  return mat + work + 3 * (size_t)N + (size_t)(N + 7) / 4 + (size_t)(N + 1) / 2 + 64;
 }
 
 struct SliceView {
@@ -189,6 +189,7 @@ struct MetroShared {
   double* xt;     // X[J_s, m] of the block at xt[s * NB + m] (16-byte aligned)
   double* yt;     // Y[m, J_s] of the block at yt[s * NB + m] (16-byte aligned)
   int* ired;      // >= 8 ints
+  uint32_t* pw;   // a^(2i+1) mod m of each site [N]: the jump-ahead to site i's first draw
   int* qj;        // accepted site of each panel column [16]
   double* qg;     // gamma of each panel column [16]
 };
@@ -482,7 +483,7 @@ __device__ __forceinline__ void metropolis_slice_blk(const HqChain& ch, double* 
   const bool log = (flags & HQ_F_LOG_RATIOS) && ch.ratios;
   // uniforms of this slice: site i consumes engine draws 2i+1, 2i+2 after the current state
   for (int i = tid; i < N; i += blockDim.x) {
-    const uint32_t x1 = minstd_mulmod(minstd_pow(2ull * i + 1), rng);
+    const uint32_t x1 = minstd_mulmod(sh.pw[i], rng);
     const uint32_t x2 = minstd_mulmod(kMinstdA, x1);
     sh.u[i] = canonical_from_pair(x1, x2);
     sh.dl[i] = sh.s[i] > 0 ? ch.delta_p : ch.delta_m;
@@ -614,6 +615,8 @@ k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int 
   sh.rr = p; p += N;
   sh.s = reinterpret_cast<int8_t*>(p);
   sh.flip = sh.s + N;
+  sh.pw = reinterpret_cast<uint32_t*>(p + (N + 7) / 4);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) sh.pw[i] = minstd_pow(2ull * i + 1);
   sh.ired = ired;
   __shared__ int qj_s[16];
   __shared__ double qg_s[16];
