@@ -109,6 +109,18 @@ __device__ inline void block_sum3(double& a, double& b, double& c, double* red) 
   c = warp_sum(lane < nw ? red[64 + lane] : 0.0);
 }
 
+// adds one slice's equal-time estimators to acc from this thread's partial sums of
+// tr = sum_i G_ii, dd = sum_i (1 - G_ii)^2 and sq = sum_ij G_ij^2 (include/observable_methods.hpp:39-83)
+__device__ inline void measure_commit(double tr, double dd, double sq, int N, double* acc, double* red) {
+  block_sum3(tr, dd, sq, red);
+  if (threadIdx.x == 0) {
+    acc[HQ_ACC_FILLING] += 2.0 - 2.0 * tr / N;
+    acc[HQ_ACC_DOCC] += dd / N;
+    acc[HQ_ACC_SWAVE] += (2.0 * sq - 2.0 * tr + N) / N;
+    acc[HQ_ACC_NSLICE] += 1.0;
+  }
+}
+
 // Element loops over an N x N column-major matrix without integer division: warps walk
 // the columns, lanes the rows (consecutive lanes touch consecutive addresses).
 #define HQ_FOR_EACH_ELEM(N, i, j)                                                      \
@@ -137,9 +149,12 @@ __device__ inline void atomic_max_double(double* addr, double val) {
 // SC selects an optional diagonal scaling fused into the pass: element (i, j) is multiplied by
 // (s[i] > 0 ? rp : rm) * (s[j] > 0 ? cp : cm), on load (SC = 1, before the convolution) or
 // on store (SC = 2); SC = 0 leaves the pass unscaled
-template <int L, int SC>
-__device__ inline void sep_pass(double* M, int ld, int N, const double* __restrict__ coef, double c, int side,
-                                int pass, const int8_t* sf, double rp, double rm, double cp, double cm) {
+// MEAS = 1 / 2 also accumulates the equal-time estimator sums of the matrix as loaded /
+// as stored (mtr, mdd, msq; see measure_commit)
+template <int L, int SC, int MEAS = 0>
+__device__ __forceinline__ void sep_pass(double* M, int ld, int N, const double* __restrict__ coef, double c, int side,
+                                int pass, const int8_t* sf, double rp, double rm, double cp, double cm,
+                                double& mtr, double& mdd, double& msq) {
   // circulant coefficients in registers (compile-time indices after unrolling)
   double a[L];
 #pragma unroll
@@ -166,6 +181,10 @@ __device__ inline void sep_pass(double* M, int ld, int N, const double* __restri
 #pragma unroll
     for (int e = 0; e < L; ++e) {
       v[e] = base[e * stride];
+      if (MEAS == 1) {
+        msq = fma(v[e], v[e], msq);
+        if (base_site + e * step_site == line) { mtr += v[e]; mdd += (1.0 - v[e]) * (1.0 - v[e]); }
+      }
       if (SC == 1) {
         const double sfac = sf[base_site + e * step_site] > 0 ? sp : sm;
         v[e] *= (side == 0) ? sfac * lf : lf * sfac;
@@ -187,35 +206,43 @@ __device__ inline void sep_pass(double* M, int ld, int N, const double* __restri
         const double sfac = sf[base_site + e * step_site] > 0 ? sp : sm;
         out *= (side == 0) ? sfac * lf : lf * sfac;
       }
+      if (MEAS == 2) {
+        msq = fma(out, out, msq);
+        if (base_site + e * step_site == line) { mtr += out; mdd += (1.0 - out) * (1.0 - out); }
+      }
       base[e * stride] = out;
     }
   }
 }
 
-// both passes of one side; SC0 / SC1 select the fused scaling of pass 0 / pass 1
-template <int L, int SC0 = 0, int SC1 = 0>
-__device__ inline void sep_apply(double* M, int ld, int N, const double* a, double c, int side,
+// both passes of one side; SC0 / SC1 select the fused scaling of pass 0 / pass 1, M0 / M1
+// the fused estimators of pass 0 / pass 1 (added to acc_meas)
+template <int L, int SC0 = 0, int SC1 = 0, int M0 = 0, int M1 = 0>
+__device__ __forceinline__ void sep_apply(double* M, int ld, int N, const double* a, double c, int side,
                                  const int8_t* sf = nullptr, double rp = 1.0, double rm = 1.0, double cp = 1.0,
-                                 double cm = 1.0) {
-  sep_pass<L, SC0>(M, ld, N, a, c, side, 0, sf, rp, rm, cp, cm);
+                                 double cm = 1.0, double* acc_meas = nullptr, double* red = nullptr) {
+  double mtr = 0.0, mdd = 0.0, msq = 0.0;
+  sep_pass<L, SC0, M0>(M, ld, N, a, c, side, 0, sf, rp, rm, cp, cm, mtr, mdd, msq);
   __syncthreads();
-  sep_pass<L, SC1>(M, ld, N, a, c, side, 1, sf, rp, rm, cp, cm);
+  sep_pass<L, SC1, M1>(M, ld, N, a, c, side, 1, sf, rp, rm, cp, cm, mtr, mdd, msq);
   __syncthreads();
+  if (M0 || M1) measure_commit(mtr, mdd, msq, N, acc_meas, red);
 }
 
 // dispatch on the lattice size to an exact compile-time fiber length (L <= HQ_MAX_L)
-template <int SC0 = 0, int SC1 = 0>
+template <int SC0 = 0, int SC1 = 0, int M0 = 0, int M1 = 0>
 __device__ __forceinline__ void sep_apply_any(double* M, int ld, int N, int L, const double* a, double c, int side,
                                      const int8_t* sf = nullptr, double rp = 1.0, double rm = 1.0,
-                                     double cp = 1.0, double cm = 1.0) {
+                                     double cp = 1.0, double cm = 1.0, double* acc_meas = nullptr,
+                                     double* red = nullptr) {
   switch (L) {
 #define HQ_SEP_CASE(n) \
-  case n: sep_apply<n, SC0, SC1>(M, ld, N, a, c, side, sf, rp, rm, cp, cm); break;
+  case n: sep_apply<n, SC0, SC1, M0, M1>(M, ld, N, a, c, side, sf, rp, rm, cp, cm, acc_meas, red); break;
     HQ_SEP_CASE(1) HQ_SEP_CASE(2) HQ_SEP_CASE(3) HQ_SEP_CASE(4) HQ_SEP_CASE(5) HQ_SEP_CASE(6)
     HQ_SEP_CASE(7) HQ_SEP_CASE(8) HQ_SEP_CASE(9) HQ_SEP_CASE(10) HQ_SEP_CASE(11) HQ_SEP_CASE(12)
     HQ_SEP_CASE(13) HQ_SEP_CASE(14) HQ_SEP_CASE(15)
 #undef HQ_SEP_CASE
-    default: sep_apply<16, SC0, SC1>(M, ld, N, a, c, side, sf, rp, rm, cp, cm); break;
+    default: sep_apply<16, SC0, SC1, M0, M1>(M, ld, N, a, c, side, sf, rp, rm, cp, cm, acc_meas, red); break;
   }
 }
 

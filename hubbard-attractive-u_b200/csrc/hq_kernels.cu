@@ -64,13 +64,7 @@ __device__ __forceinline__ void measure_slice(const double* G, int ld, int N, do
     sq = fma(v, v, sq);
     if (i == j) { tr += v; dd += (1.0 - v) * (1.0 - v); }
   }
-  block_sum3(tr, dd, sq, red);
-  if (threadIdx.x == 0) {
-    acc[HQ_ACC_FILLING] += 2.0 - 2.0 * tr / N;
-    acc[HQ_ACC_DOCC] += dd / N;
-    acc[HQ_ACC_SWAVE] += (2.0 * sq - 2.0 * tr + N) / N;
-    acc[HQ_ACC_NSLICE] += 1.0;
-  }
+  measure_commit(tr, dd, sq, N, acc, red);
 }
 
 __device__ __forceinline__ void copy_mat(double* dst, int ldd, const double* src, int lds, int N) {
@@ -530,16 +524,25 @@ __device__ __forceinline__ void metropolis_dispatch(const HqChain& ch, double* G
 //   up  : G <- e^{V_l} E G E^{-1} e^{-V_l}
 //   down: G <- E^{-1} e^{-V_l} G e^{V_l} E
 // ---------------------------------------------------------------------------------
-__device__ __forceinline__ void wrap_slice(const HqChain& ch, double* G, int ld, const int8_t* s, int dir, double* stage) {
+// With acc_meas (separable mode only) the equal-time estimators ride on the wrap: up, on the
+// first pass's loads (the G before this wrap); down, on the last pass's stores (the G after it).
+__device__ __forceinline__ void wrap_slice(const HqChain& ch, double* G, int ld, const int8_t* s, int dir, double* stage,
+                                           double* acc_meas = nullptr, double* red = nullptr) {
   const int N = ch.N;
   if (ch.expk_mode == HQK_EXPK_SEPARABLE) {
     // the e^{+-V} scalings ride on the last pass (up) or on the first pass (down)
     if (dir == HQ_UP) {
-      sep_apply_any(G, ld, N, ch.L, ch.sep_a, ch.sep_c, 0);
+      if (acc_meas)
+        sep_apply_any<0, 0, 1, 0>(G, ld, N, ch.L, ch.sep_a, ch.sep_c, 0, nullptr, 1.0, 1.0, 1.0, 1.0, acc_meas, red);
+      else
+        sep_apply_any(G, ld, N, ch.L, ch.sep_a, ch.sep_c, 0);
       sep_apply_any<0, 2>(G, ld, N, ch.L, ch.sep_ai, ch.sep_ci, 1, s, ch.ev_p, ch.ev_m, ch.ev_m, ch.ev_p);
     } else {
       sep_apply_any<1, 0>(G, ld, N, ch.L, ch.sep_ai, ch.sep_ci, 0, s, ch.ev_m, ch.ev_p, ch.ev_p, ch.ev_m);
-      sep_apply_any(G, ld, N, ch.L, ch.sep_a, ch.sep_c, 1);
+      if (acc_meas)
+        sep_apply_any<0, 0, 0, 2>(G, ld, N, ch.L, ch.sep_a, ch.sep_c, 1, nullptr, 1.0, 1.0, 1.0, 1.0, acc_meas, red);
+      else
+        sep_apply_any(G, ld, N, ch.L, ch.sep_a, ch.sep_c, 1);
     }
     return;
   }
@@ -632,13 +635,18 @@ k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int 
   __syncthreads();
 
   const int nsl = t_hi - t_lo + 1;
+  // up / down sweeps in separable mode measure inside the wrap (up: slice t's G in the wrap of
+  // slice t+1; down: in the wrap of slice t itself); the last slice of the interval is
+  // measured after stabilisation
+  const bool fused = (flags & HQ_F_MEASURE) && ch.expk_mode == HQK_EXPK_SEPARABLE &&
+                     (dir == HQ_UP || dir == HQ_DOWN);
   for (int step = 0; step < nsl; ++step) {
     const int t = (dir == HQ_DOWN) ? (t_hi - step) : (t_lo + step);
     const int l = t % ch.nt;
     for (int i = threadIdx.x; i < N; i += blockDim.x) sh.s[i] = ch.fields[(size_t)l * N + i];
     __syncthreads();
     if (dir == HQ_UP) {
-      wrap_slice(ch, G, ld, sh.s, HQ_UP, work);
+      wrap_slice(ch, G, ld, sh.s, HQ_UP, work, (fused && step > 0) ? ch.acc : nullptr, red);
       metropolis_dispatch(ch, G, ld, sh, rng, n_acc, flags, log_base);
       n_prop += N;
       log_base += N;
@@ -646,15 +654,14 @@ k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int 
       metropolis_dispatch(ch, G, ld, sh, rng, n_acc, flags, log_base);
       n_prop += N;
       log_base += N;
-      wrap_slice(ch, G, ld, sh.s, HQ_DOWN, work);
+      wrap_slice(ch, G, ld, sh.s, HQ_DOWN, work, (fused && step < nsl - 1) ? ch.acc : nullptr, red);
     } else {
       wrap_slice(ch, G, ld, sh.s, HQ_UP, work);
     }
     for (int i = threadIdx.x; i < N; i += blockDim.x) ch.fields[(size_t)l * N + i] = sh.s[i];
-    // the last slice of the interval is measured after stabilisation
     if (step < nsl - 1) {
       const int lm = (dir == HQ_DOWN) ? ((t - 1) % ch.nt) : l;
-      if (flags & HQ_F_MEASURE) measure_slice(G, ld, N, ch.acc, red);
+      if ((flags & HQ_F_MEASURE) && !fused) measure_slice(G, ld, N, ch.acc, red);
       if ((flags & HQ_F_SNAPSHOT) && ch.snap_tt) copy_mat(ch.snap_tt + (size_t)lm * N * N, N, G, ld, N);
     }
     __syncthreads();

@@ -110,11 +110,21 @@ def test_dynamic_greens_functions(hq, oracle):
     e.close()
 
 
-def test_equaltime_estimators_match_oracle(hq, oracle):
-    e, o = pair(hq, oracle, seed=11)
+@pytest.mark.parametrize("mode", [0, 1], ids=["dense", "separable"])
+def test_equaltime_estimators_match_oracle(hq, oracle, mode):
+    """Dense mode measures in a pass of its own, separable mode inside the wraps."""
+    e, o = pair(hq, oracle, seed=11, mode=mode)
     e.reset_estimators()
     e.sweep(UP, hq.SWEEP_MEASURE)
     o.sweep(UP)
+    est = e.estimators(0)
+    ref = o.measure_equaltime()
+    assert est[3] == 40
+    assert np.abs(est[:3] / est[3] - ref).max() <= 1e-10
+    # the down sweep measures inside its wraps' last passes, the up sweep in their first
+    e.reset_estimators()
+    e.sweep(DOWN, hq.SWEEP_MEASURE)
+    o.sweep(DOWN)
     est = e.estimators(0)
     ref = o.measure_equaltime()
     assert est[3] == 40
