@@ -805,7 +805,8 @@ __device__ __forceinline__ void reflector_reg(double* A, int ld, int N, int c, d
   alpha = __shfl_sync(0xffffffffu, alpha, c & 31);
   double ti = 0.0, beta = alpha;
   if (xs > 0.0) {
-    beta = -copysign(hypot(alpha, sqrt(xs)), alpha);
+    // xs is an unscaled sum of squares already, so the norm needs no hypot
+    beta = -copysign(sqrt(fma(alpha, alpha, xs)), alpha);
     ti = (beta - alpha) / beta;
     const double sc = 1.0 / (alpha - beta);
 #pragma unroll
@@ -912,10 +913,13 @@ __device__ void wy_factor(const double* A, int ld, int N, int p0, int m, const d
         if (i == j) {
           v = tau[p0 + j];
         } else if (i < j) {
-          double acc = 0.0;  // t[l] = 0 for l < i
+          double acc0 = 0.0, acc1 = 0.0;  // t[l] = 0 for l < i; two chains
 #pragma unroll
-          for (int l = 0; l < j; ++l) acc = fma(t[l], S[l * kQB + j], acc);
-          v = -tau[p0 + j] * acc;
+          for (int l = 0; l < j; l += 2) {
+            acc0 = fma(t[l], S[l * kQB + j], acc0);
+            if (l + 1 < j) acc1 = fma(t[l + 1], S[(l + 1) * kQB + j], acc1);
+          }
+          v = -tau[p0 + j] * (acc0 + acc1);
         }
       }
       t[j] = v;
