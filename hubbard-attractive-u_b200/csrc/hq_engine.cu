@@ -722,6 +722,9 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   c->desc.shrink_to_fit();
   HQ_CUDA(hq::prepare_kernels(c->Nmax, c->kmax_max, c->resident));
   HQ_CUDA(cudaMalloc(&c->d_desc, c->desc.size() * sizeof(HqChain)));
+  // the gather buffers of hq_get_estimators_all, so that no read allocates
+  HQ_CUDA(cudaMalloc(&c->d_acc_all, size_t(c->n) * HQ_ACC_COUNT * sizeof(double)));
+  HQ_CUDA(cudaMallocHost(&c->h_acc_all, size_t(c->n) * HQ_ACC_COUNT * sizeof(double)));
   upload_desc(c.get());
   build_jobs(c.get());
   HQ_CUDA(cudaStreamSynchronize(c->stream));
@@ -1023,10 +1026,6 @@ int hq_get_estimators_all(hq_ctx* c, double* out) {
   HQ_API_BEGIN
   if (!c || !out) throw HqError(HQ_E_INVALID, "null argument");
   const size_t cnt = size_t(c->n) * HQ_ACC_COUNT;
-  if (!c->d_acc_all) {
-    HQ_CUDA(cudaMalloc(&c->d_acc_all, cnt * sizeof(double)));
-    HQ_CUDA(cudaMallocHost(&c->h_acc_all, cnt * sizeof(double)));
-  }
   HQ_CUDA(hq::launch_gather_acc(c->d_desc, c->n, c->d_acc_all, c->stream));
   HQ_CUDA(cudaMemcpyAsync(c->h_acc_all, c->d_acc_all, cnt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   HQ_CUDA(cudaStreamSynchronize(c->stream));
