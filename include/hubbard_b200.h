@@ -130,8 +130,10 @@ HQ_API int hq_get_wrap_errors(hq_ctx* ctx, int chain, double* out2);
  * (include/observable_methods.hpp:39-151; divide by out[3] for the per-slice mean.) */
 HQ_API int hq_get_estimators(hq_ctx* ctx, int chain, double* out6);
 /* The same six sums for every chain at once, chain-major: out[6*chain + k]. One gather
- * launch and one device-to-host copy, instead of one copy per chain. (The reference runs
- * one chain per process and reads its estimators in place.) */
+ * launch and one device-to-host copy, instead of one copy per chain. The reference runs one
+ * chain per MPI rank and collects the ranks' results with
+ * Utils::MPI::gather_measurement_results_from_processors (include/utils/observable_gather.hpp:71);
+ * this call is the in-GPU counterpart for the chains of one context. */
 HQ_API int hq_get_estimators_all(hq_ctx* ctx, double* out);
 /* Displaced estimator sums: spin[nt], ldos[nt] and the displacement-summed
  * g(d, tau) = sum_i G(tau,0)[i+d, i] as gd[N][nt] (include/observable_methods.hpp:84-195);
