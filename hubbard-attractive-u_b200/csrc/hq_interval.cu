@@ -1,0 +1,485 @@
+// hq_interval.cu -- k_interval, the per-chain kernel of one stabilisation interval: G(tau,tau)
+// resident in shared memory while the slices of the interval are wrapped (src/dqmc_core.cpp:142-161)
+// and updated by Metropolis flips with delayed rank-k updates flushed by DMMA
+// (src/dqmc_core.cpp:102-119, src/hubbard.cpp:123-139); fused equal-time estimators
+// (include/observable_methods.hpp:39-151) and optional per-slice snapshots.
+#include "hq_common.cuh"
+
+namespace hq {
+
+// ---------------------------------------------------------------------------------
+//  Metropolis sweep over the N sites of one slice: submatrix (block-delayed) updates.
+//
+//  The reference visits i = 0..N-1 in order, draws one uniform per site, and on
+//  acceptance applies G -= gamma G[:,i] (e_i^T - G[i,:]), gamma = Delta/(1+(1-G_ii)Delta)
+//  (src/hubbard.cpp:123-139). Here the sites are taken in blocks J of NB consecutive
+//  sites (E. Gull, P. Staar, S. Fuchs et al., Submatrix updates for the continuous-time
+//  auxiliary-field algorithm, Phys. Rev. B 83, 075122 (2011), applied to the Ising HS
+//  field):
+//   1. the walk: one warp holds g = G[J, J] in registers and visits the NB sites in order
+//      with the reference's acceptance test and rank-1 updates of g alone (every later
+//      decision of the block reads only g's diagonal). For the a accepted flips
+//      j_0 < j_1 < ... it records gamma_m, X[J, m] = gamma_m g[:, j_m] and
+//      Y[m, J] = g[j_m, :] - e_{j_m}^T (g before flip m);
+//   2. the a flips become the panels of G_new = G + X Y,
+//        X[:, m] = gamma_m (G[:, j_m] + sum_{m'<m} X[:, m'] Y[m', j_m])
+//        Y[m, :] = G[j_m, :] - e_{j_m}^T + sum_{m'<m} X[j_m, m'] Y[m', :]
+//      one row of X and one column of Y per thread, with the coefficients X[J, :] and
+//      Y[:, J] from the walk's records;
+//   3. G += X Y by DMMA (rank a <= NB) over all warps.
+struct MetroShared {
+  double* dl;     // Delta of each site [N]
+  double* u;      // uniforms [N]
+  double* rr;     // visit-time ratio of each site [N] (ratio log)
+  int8_t* s;      // fields of the slice [N]
+  int8_t* flip;   // accepted flags [N]
+  double* X;      // N x 16 panel (column-major, ld panel_ld(N))
+  double* Y;      // 16 x N panel (row-major, ld panel_ld(N))
+  double* xt;     // X[J_s, m] of the block at xt[s * NB + m] (16-byte aligned)
+  double* yt;     // Y[m, J_s] of the block at yt[s * NB + m] (16-byte aligned)
+  int* ired;      // >= 8 ints
+  uint32_t* pw;   // a^(2i+1) mod m of each site [N]: the jump-ahead to site i's first draw
+  int* qj;        // accepted site of each panel column [16]
+  double* qg;     // gamma of each panel column [16]
+};
+
+// the walk of the block [b0, b0 + nb) by one warp (see above); writes the records, the
+// accepted count into ired[slot] and the two triangular factors
+template <int NB>
+__device__ __forceinline__ void walk_block(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0, int nb,
+                           bool log, int slot, double& acc_count) {
+  constexpr int R = (NB * NB >= 32) ? NB * NB / 32 : 1;  // rows of g held by one lane
+  constexpr int H = NB / R;                              // lane groups (rows h*R .. h*R+R-1)
+  const int lane = threadIdx.x & 31;
+  // lane layout of g: lane le = h * NB + c holds g[h*R + i][c], i < R (lanes >= NB*H mirror)
+  const int le = lane % (NB * H), c = le % NB, h = le / NB;
+  const bool writer = lane < NB * H;
+  double r[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int row = h * R + i;
+    r[i] = (row < nb && c < nb) ? G[b0 + row + (size_t)(b0 + c) * ld] : 0.0;
+  }
+  // per-site constants of the block, loaded before the walk (the walk's shared-memory
+  // stores would otherwise order every later load behind them)
+  double dls[NB], thr[NB];
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    dls[s] = s < nb ? sh.dl[b0 + s] : 0.0;
+    thr[s] = s < nb ? sh.u[b0 + s] * (1.0 + dls[s]) : 0.0;
+  }
+  // per-site records stay in registers during the walk (shared-memory stores would queue
+  // with the shuffles on the same pipe): xk[s] = X[J_row, s] for the row this lane writes,
+  // yk[s] = Y[s, J_c], the acceptance mask and, in lane s, gamma_s and the visit ratio
+  double xk[NB], yk[NB], myg = 0.0, myr = 0.0;
+  unsigned mask = 0u;
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    xk[s] = 0.0;
+    yk[s] = 0.0;
+    if (s < nb) {
+      const int ss = s / R, si = s % R;  // g[s][*] is held by group ss at register si
+      // column s, row s and the diagonal entry of the current g; gamma is formed before
+      // the decision so that its division overlaps the test
+      const double dg = __shfl_sync(0xffffffffu, r[si], ss * NB + s);
+      double colr[R];
+#pragma unroll
+      for (int i = 0; i < R; ++i) colr[i] = __shfl_sync(0xffffffffu, r[i], h * NB + s);
+      const double yv = __shfl_sync(0xffffffffu, r[si], ss * NB + c) - (c == s ? 1.0 : 0.0);
+      const double dl = dls[s];
+      const double av = 1.0 + (1.0 - dg) * dl;
+      const double gam = dl / av;
+      if (log && lane == s) myr = (av * av) / (1.0 + dl);
+      // accept iff u < min(1, |r|), r = a^2 / (1 + Delta), 1 + Delta = e^{-2 alpha s} > 0
+      const bool acc = thr[s] < av * av;
+      const double ge = acc ? gam : 0.0;
+      double xs = colr[0];
+#pragma unroll
+      for (int i = 1; i < R; ++i) xs = (c == i) ? colr[i] : xs;
+      xk[s] = ge * xs;
+      yk[s] = yv;
+      if (lane == s) myg = gam;
+#pragma unroll
+      for (int i = 0; i < R; ++i) r[i] = fma(ge * colr[i], yv, r[i]);
+      mask |= acc ? (1u << s) : 0u;
+    }
+  }
+  // the records of the accepted flips, in acceptance order
+  const int a = __popc(mask);
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    if (mask & (1u << s)) {
+      const int m = __popc(mask & ((1u << s) - 1u));
+      if (writer && c < R) sh.xt[(h * R + c) * NB + m] = xk[s];
+      if (writer && h == 0) sh.yt[c * NB + m] = yk[s];
+    }
+  }
+  if (lane < nb) {
+    const bool acc = (mask >> lane) & 1u;
+    if (acc) {
+      const int m = __popc(mask & ((1u << lane) - 1u));
+      sh.qj[m] = b0 + lane;
+      sh.qg[m] = myg;
+    }
+    sh.flip[b0 + lane] = acc ? 1 : 0;
+    if (log) sh.rr[b0 + lane] = myr;
+  }
+  if (lane == 0) sh.ired[slot] = a;
+  acc_count += (lane == 0) ? (double)a : 0.0;
+}
+
+// the walk of a 16-site block with g tiled 4 rows x 2 columns per lane: lane 8 rg + cg holds
+// g[4 rg + a][2 cg + b] (a < 4, b < 2). A step needs column s for the lane's four rows, row s
+// for its two columns and the diagonal entry: 7 shuffles instead of the 10 of an 8 x 1 tile.
+// Every entry is updated with the same expression as in walk_block, so the two walks agree
+// bitwise. Records: lanes with cg < 4 write X[J_(4 rg + cg), m], lanes with rg < 2 write
+// Y[m, J_(2 cg + rg)].
+__device__ __forceinline__ void walk_block16(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0,
+                                             int nb, bool log, int slot, double& acc_count) {
+  constexpr int NB = 16;
+  const int lane = threadIdx.x & 31;
+  const int rg = lane >> 3, cg = lane & 7;
+  double r[4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int row = 4 * rg + a, col = 2 * cg + b;
+      r[a][b] = (row < nb && col < nb) ? G[b0 + row + (size_t)(b0 + col) * ld] : 0.0;
+    }
+  double dls[NB], thr[NB];
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    dls[s] = s < nb ? sh.dl[b0 + s] : 0.0;
+    thr[s] = s < nb ? sh.u[b0 + s] * (1.0 + dls[s]) : 0.0;
+  }
+  double xk[NB], yk[NB], myg = 0.0, myr = 0.0;
+  unsigned mask = 0u;
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    xk[s] = 0.0;
+    yk[s] = 0.0;
+    if (s < nb) {
+      // g[s][s]; column s at the lane's rows (held by lane 8 rg + s/2, column slot s&1);
+      // row s at the lane's columns (held by lane 8 (s/4) + cg, row slot s&3)
+      const double dg = __shfl_sync(0xffffffffu, r[s & 3][s & 1], 8 * (s >> 2) + (s >> 1));
+      double colr[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) colr[a] = __shfl_sync(0xffffffffu, r[a][s & 1], 8 * rg + (s >> 1));
+      double rowv[2];
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        rowv[b] = __shfl_sync(0xffffffffu, r[s & 3][b], 8 * (s >> 2) + cg) - (2 * cg + b == s ? 1.0 : 0.0);
+      const double dl = dls[s];
+      const double av = 1.0 + (1.0 - dg) * dl;
+      const double gam = dl / av;
+      if (log && lane == s) myr = (av * av) / (1.0 + dl);
+      const bool acc = thr[s] < av * av;
+      const double ge = acc ? gam : 0.0;
+      // the record row of this lane is 4 rg + cg (cg < 4), its record column 2 cg + rg (rg < 2)
+      double xs = colr[0];
+      xs = (cg == 1) ? colr[1] : xs;
+      xs = (cg == 2) ? colr[2] : xs;
+      xs = (cg == 3) ? colr[3] : xs;
+      xk[s] = ge * xs;
+      yk[s] = (rg & 1) ? rowv[1] : rowv[0];
+      if (lane == s) myg = gam;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const double f = ge * colr[a];
+#pragma unroll
+        for (int b = 0; b < 2; ++b) r[a][b] = fma(f, rowv[b], r[a][b]);
+      }
+      mask |= acc ? (1u << s) : 0u;
+    }
+  }
+  const int a = __popc(mask);
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    if (mask & (1u << s)) {
+      const int m = __popc(mask & ((1u << s) - 1u));
+      if (cg < 4) sh.xt[(4 * rg + cg) * NB + m] = xk[s];
+      if (rg < 2) sh.yt[(2 * cg + rg) * NB + m] = yk[s];
+    }
+  }
+  if (lane < nb) {
+    const bool acc = (mask >> lane) & 1u;
+    if (acc) {
+      const int m = __popc(mask & ((1u << lane) - 1u));
+      sh.qj[m] = b0 + lane;
+      sh.qg[m] = myg;
+    }
+    sh.flip[b0 + lane] = acc ? 1 : 0;
+    if (log) sh.rr[b0 + lane] = myr;
+  }
+  if (lane == 0) sh.ired[slot] = a;
+  acc_count += (lane == 0) ? (double)a : 0.0;
+}
+
+// panels of the a flips of block [b0, b0 + NB): the two triangular recurrences, one row of X
+// and one column of Y per thread; the coefficients of flip m are contiguous in the records
+// (xt / yt at row j_m - b0) and are read in 16-byte pairs
+template <int NB>
+__device__ __forceinline__ void build_panels(const double* G, int ld, int N, const MetroShared& sh, int ldp, int a, int b0) {
+  for (int p = threadIdx.x; p < N; p += blockDim.x) {
+    double x[NB], y[NB];
+#pragma unroll
+    for (int m = 0; m < NB; ++m) {
+      x[m] = 0.0;
+      y[m] = 0.0;
+      if (m < a) {
+        const int jm = sh.qj[m], sj = jm - b0;
+        const double* cy = sh.yt + sj * NB;  // Y[m2, j_m]
+        const double* cx = sh.xt + sj * NB;  // X[j_m, m2]
+        double cx0 = G[p + (size_t)jm * ld], cx1 = 0.0;
+        double cy0 = G[jm + (size_t)p * ld] - (p == jm ? 1.0 : 0.0), cy1 = 0.0;
+#pragma unroll
+        for (int m2 = 0; m2 + 1 < m; m2 += 2) {
+          const double2 vy = *reinterpret_cast<const double2*>(cy + m2);
+          const double2 vx = *reinterpret_cast<const double2*>(cx + m2);
+          cx0 = fma(x[m2], vy.x, cx0);
+          cx1 = fma(x[m2 + 1], vy.y, cx1);
+          cy0 = fma(vx.x, y[m2], cy0);
+          cy1 = fma(vx.y, y[m2 + 1], cy1);
+        }
+        if (m & 1) {
+          cx0 = fma(x[m - 1], cy[m - 1], cx0);
+          cy0 = fma(cx[m - 1], y[m - 1], cy0);
+        }
+        x[m] = sh.qg[m] * (cx0 + cx1);
+        y[m] = cy0 + cy1;
+      }
+    }
+    // stores after the recurrence: the loads above are free to run ahead of them
+#pragma unroll
+    for (int m = 0; m < NB; ++m) {
+      if (m < a) {
+        sh.X[p + m * ldp] = x[m];
+        sh.Y[m * ldp + p] = y[m];
+      }
+    }
+  }
+}
+
+// G[0:M, 0:Nc] += X[:, 0:k] Y[0:k, :] (k <= 16): 48 x 32 warp tiles (3 x 4 DMMA tiles sharing
+// their fragments; 144 = 3 x 48), all warps
+__device__ __forceinline__ void rank_update48(double* G, int ld, int M, int Nc, const double* X, int ldx, const double* Y, int ldy,
+                              int k) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int mt = (M + 47) / 48, ns = (Nc + 31) / 32;
+  const int ksteps = (k + 3) >> 2;
+  for (int st = warp; st < mt * ns; st += nw) {
+    const int r0 = (st % mt) * 48, c0 = (st / mt) * 32;
+    double acc[3][4][4];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int r = r0 + 16 * i + g, c = c0 + t * 8 + 2 * q;
+        acc[i][t][0] = (r < M && c < Nc) ? G[r + (size_t)c * ld] : 0.0;
+        acc[i][t][1] = (r < M && c + 1 < Nc) ? G[r + (size_t)(c + 1) * ld] : 0.0;
+        acc[i][t][2] = (r + 8 < M && c < Nc) ? G[r + 8 + (size_t)c * ld] : 0.0;
+        acc[i][t][3] = (r + 8 < M && c + 1 < Nc) ? G[r + 8 + (size_t)(c + 1) * ld] : 0.0;
+      }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      if (s < ksteps) {
+        const int m = 4 * s + q;
+        const bool mk = m < k;
+        double fa[3][2], fb[4];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const int r = r0 + 16 * i + g;
+          fa[i][0] = (r < M && mk) ? X[r + m * ldx] : 0.0;
+          fa[i][1] = (r + 8 < M && mk) ? X[r + 8 + m * ldx] : 0.0;
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int cb = c0 + t * 8 + g;
+          fb[t] = (cb < Nc && mk) ? Y[m * ldy + cb] : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int t = 0; t < 4; ++t) dmma_16x8x4(acc[i][t], fa[i][0], fa[i][1], fb[t]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int r = r0 + 16 * i + g, c = c0 + t * 8 + 2 * q;
+        if (r < M && c < Nc) G[r + (size_t)c * ld] = acc[i][t][0];
+        if (r < M && c + 1 < Nc) G[r + (size_t)(c + 1) * ld] = acc[i][t][1];
+        if (r + 8 < M && c < Nc) G[r + 8 + (size_t)c * ld] = acc[i][t][2];
+        if (r + 8 < M && c + 1 < Nc) G[r + 8 + (size_t)(c + 1) * ld] = acc[i][t][3];
+      }
+  }
+}
+
+// the flush of one block's flips, G[0:N, 0:N] += X[:, 0:k] Y[0:k, :]
+__device__ __forceinline__ void flush_block(double* G, int ld, int N, const double* X, int ldx, const double* Y, int ldy, int k) {
+  rank_update48(G, ld, N, N, X, ldx, Y, ldy, k);
+}
+
+template <int NB>
+__device__ __forceinline__ void metropolis_slice_blk(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
+                                     double& n_acc, int flags, long long log_base) {
+  const int N = ch.N;
+  const int ldp = panel_ld(N);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const bool log = (flags & HQ_F_LOG_RATIOS) && ch.ratios;
+  // uniforms of this slice: site i consumes engine draws 2i+1, 2i+2 after the current state
+  for (int i = tid; i < N; i += blockDim.x) {
+    const uint32_t x1 = minstd_mulmod(sh.pw[i], rng);
+    const uint32_t x2 = minstd_mulmod(kMinstdA, x1);
+    sh.u[i] = canonical_from_pair(x1, x2);
+    sh.dl[i] = sh.s[i] > 0 ? ch.delta_p : ch.delta_m;
+    sh.flip[i] = 0;
+  }
+  rng = minstd_mulmod(minstd_pow(2ull * N), rng);
+  __syncthreads();
+  double acc_count = 0.0;
+  for (int b0 = 0, bi = 0; b0 < N; b0 += NB, ++bi) {
+    if (warp == 0) {
+      if constexpr (NB == 16) walk_block16(ch, G, ld, sh, b0, min(NB, N - b0), log, bi & 1, acc_count);
+      else walk_block<NB>(ch, G, ld, sh, b0, min(NB, N - b0), log, bi & 1, acc_count);
+    }
+    __syncthreads();
+    // the count alternates between two words: with no flush (a == 0) no barrier follows,
+    // and warp 0 writes the next block's count while other warps may still read this one
+    const int a = sh.ired[bi & 1];
+    if (a == 0) continue;
+    build_panels<NB>(G, ld, N, sh, ldp, a, b0);
+    __syncthreads();
+    flush_block(G, ld, N, sh.X, ldp, sh.Y, ldp, a);
+    __syncthreads();
+  }
+  __syncthreads();
+  n_acc += acc_count;
+  // apply the flips of this slice and optionally log the visit-time ratios
+  for (int i = tid; i < N; i += blockDim.x) {
+    if (sh.flip[i]) sh.s[i] = -sh.s[i];
+    if (log && log_base + i < ch.ratio_cap) ch.ratios[log_base + i] = sh.rr[i];
+  }
+  __syncthreads();
+}
+
+// block size NB of the submatrix updates: the chain's delay depth (4, 8 or 16)
+__device__ __forceinline__ void metropolis_dispatch(const HqChain& ch, double* G, int ld, const MetroShared& sh, uint32_t& rng,
+                                    double& n_acc, int flags, long long log_base) {
+  if (ch.kmax >= 16) metropolis_slice_blk<16>(ch, G, ld, sh, rng, n_acc, flags, log_base);
+  else if (ch.kmax >= 8) metropolis_slice_blk<8>(ch, G, ld, sh, rng, n_acc, flags, log_base);
+  else metropolis_slice_blk<4>(ch, G, ld, sh, rng, n_acc, flags, log_base);
+}
+
+// ---------------------------------------------------------------------------------
+//  k_interval: the update (or no-update) slices of one stabilisation interval.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(HQ_INT_THREADS, 1)
+k_interval(const HqChain* __restrict__ chains, int nchains, int dir, int b, int flags, int resident) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ HqChain ch;
+  __shared__ double red[96];
+  __shared__ int ired[64];
+  const int c = blockIdx.x;
+  if (c >= nchains) return;
+  if (threadIdx.x == 0) ch = chains[c];
+  __syncthreads();
+  if (!ch.active || b >= ch.n_stab) return;
+  const int N = ch.N;
+  int t_lo, t_hi;
+  interval_range(ch.nt, ch.pace, ch.n_stab, dir, b, t_lo, t_hi);
+
+  // shared-memory carve-up
+  double* p = smem;
+  double* G;
+  int ld;
+  if (resident) {
+    G = p;
+    ld = interval_ld(N);
+    p += (size_t)N * ld;
+    load_mat_async(G, ld, ch.G, N, N);
+  } else {
+    G = ch.G;
+    ld = N;
+  }
+  const size_t panels = (size_t)panel_ld(N) * ch.kmax * 2;
+  const size_t stage_n = (size_t)8 * (((N + 15) & ~15) + 4);
+  double* work = p;
+  p += panels > stage_n ? panels : stage_n;
+  MetroShared sh;
+  sh.X = work;
+  sh.Y = work + (size_t)panel_ld(N) * ch.kmax;
+  sh.dl = p; p += N;
+  sh.u = p; p += N;
+  sh.rr = p; p += N;
+  sh.s = reinterpret_cast<int8_t*>(p);
+  sh.flip = sh.s + N;
+  sh.pw = reinterpret_cast<uint32_t*>(p + (N + 7) / 4);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) sh.pw[i] = minstd_pow(2ull * i + 1);
+  sh.ired = ired;
+  __shared__ int qj_s[16];
+  __shared__ double qg_s[16];
+  __shared__ __align__(16) double xt_s[16 * 16];
+  __shared__ __align__(16) double yt_s[16 * 16];
+  sh.qj = qj_s;
+  sh.qg = qg_s;
+  sh.xt = xt_s;
+  sh.yt = yt_s;
+  uint32_t rng = *ch.rng;
+  double n_acc = 0.0, n_prop = 0.0;
+  long long log_base = (flags & HQ_F_LOG_RATIOS) && ch.ratio_count ? *ch.ratio_count : 0;
+  __syncthreads();
+
+  const int nsl = t_hi - t_lo + 1;
+  // up / down sweeps in separable mode measure inside the wrap (up: slice t's G in the wrap of
+  // slice t+1; down: in the wrap of slice t itself); the last slice of the interval is
+  // measured after stabilisation
+  const bool fused = (flags & HQ_F_MEASURE) && ch.expk_mode == HQK_EXPK_SEPARABLE &&
+                     (dir == HQ_UP || dir == HQ_DOWN);
+  for (int step = 0; step < nsl; ++step) {
+    const int t = (dir == HQ_DOWN) ? (t_hi - step) : (t_lo + step);
+    const int l = t % ch.nt;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) sh.s[i] = ch.fields[(size_t)l * N + i];
+    __syncthreads();
+    if (dir == HQ_UP) {
+      wrap_slice(ch, G, ld, sh.s, HQ_UP, work, (fused && step > 0) ? ch.acc : nullptr, red);
+      metropolis_dispatch(ch, G, ld, sh, rng, n_acc, flags, log_base);
+      n_prop += N;
+      log_base += N;
+    } else if (dir == HQ_DOWN) {
+      metropolis_dispatch(ch, G, ld, sh, rng, n_acc, flags, log_base);
+      n_prop += N;
+      log_base += N;
+      wrap_slice(ch, G, ld, sh.s, HQ_DOWN, work, (fused && step < nsl - 1) ? ch.acc : nullptr, red);
+    } else {
+      wrap_slice(ch, G, ld, sh.s, HQ_UP, work);
+    }
+    for (int i = threadIdx.x; i < N; i += blockDim.x) ch.fields[(size_t)l * N + i] = sh.s[i];
+    if (step < nsl - 1) {
+      const int lm = (dir == HQ_DOWN) ? ((t - 1) % ch.nt) : l;
+      if ((flags & HQ_F_MEASURE) && !fused) measure_slice(G, ld, N, ch.acc, red);
+      if ((flags & HQ_F_SNAPSHOT) && ch.snap_tt) copy_mat(ch.snap_tt + (size_t)lm * N * N, N, G, ld, N);
+    }
+    __syncthreads();
+  }
+  if (resident) copy_mat(ch.G, N, G, ld, N);
+  if (threadIdx.x == 0) {
+    *ch.rng = rng;
+    ch.acc[HQ_ACC_PROPOSED] += n_prop;
+    ch.acc[HQ_ACC_ACCEPTED] += n_acc;
+    if ((flags & HQ_F_LOG_RATIOS) && ch.ratio_count) *ch.ratio_count = log_base;
+  }
+}
+
+cudaError_t launch_interval(const HqChain* chains, int n, int dir, int b, int flags, int Nmax, int kmax, bool resident,
+                            cudaStream_t st) {
+  const size_t bytes = smem_interval_bytes(Nmax, kmax, resident);
+  k_interval<<<n, HQ_INT_THREADS, bytes, st>>>(chains, n, dir, b, flags, resident ? 1 : 0);
+  return cudaGetLastError();
+}
+const void* fn_interval() { return (const void*)k_interval; }
+
+}  // namespace hq

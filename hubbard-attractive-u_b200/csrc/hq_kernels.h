@@ -25,6 +25,10 @@ cudaError_t launch_dyn_measure(const HqChain* chains, int n, int b, int last_onl
 cudaError_t launch_dyn_store(const HqChain* chains, int n, int b, cudaStream_t st);
 cudaError_t launch_dyn_commit(const HqChain* chains, int n, int b, cudaStream_t st);
 cudaError_t launch_gather_acc(const HqChain* chains, int n, double* out, cudaStream_t st);
+// the per-chain kernels that live in their own translation units (for function attributes)
+const void* fn_interval();
+const void* fn_udt();
+const void* fn_invert();
 cudaError_t launch_adj_interval(const HqChain* chains, int n, int b, int Nmax, bool resident, cudaStream_t st);
 cudaError_t launch_adj_last(const HqChain* chains, int n, int b, cudaStream_t st);
 }  // namespace hq
