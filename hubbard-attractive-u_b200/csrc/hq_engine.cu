@@ -7,11 +7,13 @@
 // fixed sequence of kernel launches on one stream (optionally captured in a CUDA graph).
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <tuple>
@@ -1370,14 +1372,14 @@ int hq_logdet_adjoint(hq_ctx* c, double* out, double* logdet) {
 // =======================================================================================
 //  hq_equaltime_g_noalloc: an entry point that allocates no device memory.
 //
-//  Some callers cannot call cudaMalloc: code that runs inside a region being captured into
-//  a CUDA graph by someone else, runtimes that hand out a fixed pool of device memory up
-//  front and forbid further allocations, or embedded hosts that must never fail on an
-//  out-of-memory path after start-up. For them, hq_equaltime_g_noalloc computes the
-//  equal-time Green's function G(0,0) = (1 + B(nt-1)...B(0))^-1 of one chain from Ising
-//  fields already on the device, with every temporary (the UDV stack, the work matrices,
-//  the chain descriptor and the GEMM job lists) held in one file-scope device array of
-//  fixed size. The work is the kernel sequence of hq_init_stacks_and_g.
+//  Some callers cannot call cudaMalloc: a process that hands out its whole device-memory
+//  budget once at start-up and forbids allocations after that, or a long-running service
+//  that must never meet an out-of-memory failure in the middle of its work. For them,
+//  hq_equaltime_g_noalloc computes the equal-time Green's function
+//  G(0,0) = (1 + B(nt-1)...B(0))^-1 of one chain from Ising fields already on the device,
+//  with every temporary (the UDV stack, the work matrices, the chain descriptor and the GEMM
+//  job lists) held in one file-scope device array of fixed size. The work is the kernel
+//  sequence of hq_init_stacks_and_g.
 // =======================================================================================
 namespace {
 
@@ -1389,7 +1391,10 @@ constexpr int kMaxStab = 16;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {nullptr};  // device address of the scratch, per device
+// device address of the scratch, looked up once per device (with that device current) by the
+// first call on it; valid for the life of the device's context
+std::atomic<void*> g_scratch_addr[kMaxDevices];
+std::mutex g_scratch_mutex;
 
 int set_error(int code, const std::string& msg) {
   g_last_error = msg;  // reported by hq_last_error()
@@ -1404,8 +1409,8 @@ HqGemmJob job(int N, const double* A, int ta, const double* B, int tb, double* C
 
 }  // namespace
 
-extern "C" HQ_API int hq_equaltime_g_noalloc(int nl, double nnt, double u, double mu, double beta, int nt, int pace,
-                                             const signed char* fields_dev, double* g_dev, void* stream) {
+static int equaltime_g_noalloc(int nl, double nnt, double u, double mu, double beta, int nt, int pace,
+                               const signed char* fields_dev, double* g_dev, void* stream) {
   // ---- argument and size checks (include/dqmc_parser.hpp:124-132 plus the scratch limits) ----
   if (!fields_dev || !g_dev) return set_error(HQ_E_INVALID, "hq_equaltime_g_noalloc: null device pointer");
   if (nl < 1 || nt < 1 || pace < 1 || u < 0 || beta < 0)
@@ -1423,15 +1428,21 @@ extern "C" HQ_API int hq_equaltime_g_noalloc(int nl, double nnt, double u, doubl
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return set_error(HQ_E_CUDA, "hq_equaltime_g_noalloc: no current CUDA device");
   // ---- set-up, once per device, with that device current: the scratch's device address ----
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return set_error(HQ_E_CUDA, std::string("hq_equaltime_g_noalloc: cudaGetSymbolAddress: ") +
-                                      cudaGetErrorString(e));
-    g_scratch_addr[dev] = p;
+  void* addr = g_scratch_addr[dev].load(std::memory_order_acquire);
+  if (!addr) {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    addr = g_scratch_addr[dev].load(std::memory_order_relaxed);
+    if (!addr) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p)
+        return set_error(HQ_E_CUDA, std::string("hq_equaltime_g_noalloc: cudaGetSymbolAddress: ") +
+                                        cudaGetErrorString(e));
+      g_scratch_addr[dev].store(p, std::memory_order_release);
+      addr = p;
+    }
   }
-  char* base = static_cast<char*>(g_scratch_addr[dev]);
+  char* base = static_cast<char*>(addr);
 
   // ---- scratch layout ----
   const size_t NN = size_t(N) * N, mat = NN * sizeof(double);
@@ -1555,4 +1566,17 @@ extern "C" HQ_API int hq_equaltime_g_noalloc(int nl, double nnt, double u, doubl
   if (e == cudaSuccess) e = hq::launch_gemm(d_jobs + jb + 3, 1, N, N, st);
   if (e != cudaSuccess) return set_error(HQ_E_CUDA, std::string("hq_equaltime_g_noalloc: launch: ") + cudaGetErrorString(e));
   return HQ_OK;
+}
+
+// The C entry point: host-side failures (a std::bad_alloc of the small host vectors, say)
+// become status codes instead of crossing the C ABI as exceptions.
+extern "C" HQ_API int hq_equaltime_g_noalloc(int nl, double nnt, double u, double mu, double beta, int nt, int pace,
+                                             const signed char* fields_dev, double* g_dev, void* stream) {
+  try {
+    return equaltime_g_noalloc(nl, nnt, u, mu, beta, nt, pace, fields_dev, g_dev, stream);
+  } catch (const std::bad_alloc&) {
+    return set_error(HQ_E_NOMEM, "hq_equaltime_g_noalloc: host allocation failed");
+  } catch (const std::exception& e) {
+    return set_error(HQ_E_INVALID, std::string("hq_equaltime_g_noalloc: ") + e.what());
+  }
 }

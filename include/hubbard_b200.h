@@ -211,17 +211,22 @@ HQ_API int hq_upload_fields_i8(hq_ctx* ctx, const signed char* fields_all);
 HQ_API int hq_download_fields_i8(hq_ctx* ctx, signed char* fields_all);
 
 /* Equal-time G(0,0) = (1 + B(nt-1)...B(0))^-1 of one chain, computed without allocating any
- * device memory, for callers that cannot call cudaMalloc (inside someone else's stream
- * capture, under a fixed device-memory budget handed out up front, or on hosts that must
- * not meet an out-of-memory path after start-up). No counterpart in the reference.
+ * device memory. No counterpart in the reference: it serves callers that cannot call
+ * cudaMalloc, such as a process that hands out its whole device-memory budget once at start-up
+ * and forbids allocations after that, or a long-running service that must never meet an
+ * out-of-memory failure in the middle of its work.
  *   fields_dev: device array of nt*N int8 fields (+1/-1, [nt][N]); g_dev: device output,
  *   N*N doubles, column-major; stream: cudaStream_t (NULL = default stream).
  * Limits: N = nl*nl <= 64 and ceil(nt / stabilization_pace) <= 16; larger sizes return
  * HQ_E_RANGE with a message in hq_last_error(). All temporaries live in one 4 MiB device
- * array defined in the library, which every GPU that loads the library keeps until exit;
- * its first call on a device looks up that array's device address and raises the
- * kernels' shared-memory limits where needed (call it once before any stream capture). Calls share the array: calls that overlap on the GPU race, so
- * serialise them (one stream, or stream ordering). The work is enqueued on `stream`. */
+ * array defined in the library, which every GPU that loads the library keeps until exit.
+ * The first call on a device does the set-up: it looks up that array's device address (with
+ * the device current) and raises the kernels' shared-memory limits where needed, so make the
+ * first call on each device before any stream capture. The address is kept for the life of
+ * the device's context: do not call it again on a device after cudaDeviceReset. Every call
+ * shares the array and the array keeps the last call's contents: calls that overlap on the
+ * GPU race, so serialise them (one stream, or stream ordering). The work is enqueued on
+ * `stream`. */
 HQ_API int hq_equaltime_g_noalloc(int nl, double nnt, double u, double mu, double beta, int nt,
                                   int stabilization_pace, const signed char* fields_dev, double* g_dev,
                                   void* stream);
