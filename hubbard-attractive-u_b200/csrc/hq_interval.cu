@@ -43,6 +43,26 @@ struct MetroShared {
   double* qg;     // gamma of each panel column [16]
 };
 
+// The acceptance ratio exactly as the reference evaluates it (src/hubbard.cpp:123-130):
+// r = (1 + (1 - G_ii) Delta)^2 / (1 + Delta), each operation rounded on its own (no FMA
+// contraction), the square as one product.
+__device__ __forceinline__ double reference_ratio(double gii, double dl) {
+  const double a = __dadd_rn(1.0, __dmul_rn(__dadd_rn(1.0, -gii), dl));
+  return __ddiv_rn(__dmul_rn(a, a), __dadd_rn(1.0, dl));
+}
+
+// The Metropolis decision of src/dqmc_core.cpp:110: accept iff u < min(1, |r|). The walk
+// tests u (1 + Delta) < a^2 (thr = u (1 + Delta), 1 + Delta > 0), which needs no division on
+// its dependency chain and equals the reference's test except when the two sides lie within
+// a few rounding errors of each other; there (thr and a are the same in every lane, so the
+// branch is warp-uniform, and it is taken with probability ~1e-12) the reference's own form
+// decides, with the uniform read back from shared memory.
+__device__ __forceinline__ bool accept_flip(double thr, double av, double gii, double dl, const double* u) {
+  const double a2 = av * av;
+  if (fabs(thr - a2) > 1e-12 * a2) return thr < a2;
+  return *u < fmin(1.0, fabs(reference_ratio(gii, dl)));
+}
+
 // the walk of the block [b0, b0 + nb) by one warp (see above); writes the records, the
 // accepted count into ired[slot] and the two triangular factors
 template <int NB>
@@ -89,9 +109,9 @@ __device__ __forceinline__ void walk_block(const HqChain& ch, const double* G, i
       const double dl = dls[s];
       const double av = 1.0 + (1.0 - dg) * dl;
       const double gam = dl / av;
-      if (log && lane == s) myr = (av * av) / (1.0 + dl);
+      if (log && lane == s) myr = reference_ratio(dg, dl);
       // accept iff u < min(1, |r|), r = a^2 / (1 + Delta), 1 + Delta = e^{-2 alpha s} > 0
-      const bool acc = thr[s] < av * av;
+      const bool acc = accept_flip(thr[s], av, dg, dl, sh.u + b0 + s);
       const double ge = acc ? gam : 0.0;
       double xs = colr[0];
 #pragma unroll
@@ -173,8 +193,8 @@ __device__ __forceinline__ void walk_block16(const HqChain& ch, const double* G,
       const double dl = dls[s];
       const double av = 1.0 + (1.0 - dg) * dl;
       const double gam = dl / av;
-      if (log && lane == s) myr = (av * av) / (1.0 + dl);
-      const bool acc = thr[s] < av * av;
+      if (log && lane == s) myr = reference_ratio(dg, dl);
+      const bool acc = accept_flip(thr[s], av, dg, dl, sh.u + b0 + s);
       const double ge = acc ? gam : 0.0;
       // the record row of this lane is 4 rg + cg (cg < 4), its record column 2 cg + rg (rg < 2)
       double xs = colr[0];

@@ -450,6 +450,11 @@ struct Core {
   long long n_proposed = 0, n_accepted = 0;
   // optional replay log: every acceptance ratio in visiting order
   std::vector<double>* ratio_log = nullptr;
+  // optional forced trajectory (test infrastructure, not in the reference): when set, site
+  // (t, i) flips iff forced[t*ns + i] differs from its current field; the random draw of
+  // the reference is still consumed. It replays another implementation's field trajectory
+  // so that its G's can be compared at any stabilisation pace.
+  const std::vector<int>* forced = nullptr;
 
   void initialize(const Params& p) {
     ns = p.ns; nt = p.nt; pace = p.pace; is_equaltime = p.is_equaltime; is_dynamic = p.is_dynamic;
@@ -479,7 +484,9 @@ struct Core {
       const double r = model.acceptance_ratio(gftt, t, i);
       if (ratio_log) ratio_log->push_back(r);
       ++n_proposed;
-      if (std::bernoulli_distribution(std::min(1.0, std::abs(r)))(*eng)) {
+      bool accept = std::bernoulli_distribution(std::min(1.0, std::abs(r)))(*eng);
+      if (forced) accept = (*forced)[size_t(t) * ns + i] != model.s(t, i);
+      if (accept) {
         model.update_green_function(gftt, t, i);
         model.s(t, i) = -model.s(t, i);  // src/hubbard.cpp:118-121
         ++n_accepted;
@@ -678,7 +685,12 @@ void* or_create(int nl, double nnt, double u, double mu, double beta, int nt, in
     return c;
   } catch (...) { return nullptr; }
 }
-void or_destroy(void* h) { delete static_cast<Chain*>(h); }
+void or_destroy(void* h) {
+  auto* c = static_cast<Chain*>(h);
+  delete c->core.forced;
+  delete c->core.ratio_log;
+  delete c;
+}
 double or_alpha(void* h) { return static_cast<Chain*>(h)->model.alpha; }
 void or_get_expk(void* h, double* expk, double* inv_expk) {
   auto* c = static_cast<Chain*>(h);
@@ -705,6 +717,12 @@ int or_init(void* h) {
     c->core.current_t = 0;
     return 0;
   } catch (...) { return -1; }
+}
+// forced field trajectory (see Core::forced): target [nt][ns] or NULL to return to Metropolis
+void or_set_forced_fields(void* h, const int* target) {
+  auto* c = static_cast<Chain*>(h);
+  delete c->core.forced;
+  c->core.forced = target ? new std::vector<int>(target, target + size_t(c->p.nt) * c->p.ns) : nullptr;
 }
 void or_set_thermalization(void* h, int on) { static_cast<Chain*>(h)->core.is_thermalization = on; }
 int or_sweep(void* h, int dir) {

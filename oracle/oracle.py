@@ -38,6 +38,7 @@ def lib():
         L.or_init.restype = i
         L.or_init.argtypes = [vp]
         L.or_set_thermalization.argtypes = [vp, i]
+        L.or_set_forced_fields.argtypes = [vp, ip]
         L.or_sweep.restype = i
         L.or_sweep.argtypes = [vp, i]
         L.or_current_g.argtypes = [vp, dp]
@@ -133,6 +134,15 @@ class OracleChain:
     def init(self):
         if lib().or_init(self.h) != 0:
             raise RuntimeError("or_init failed")
+
+    def force_fields(self, target):
+        """Replays a given field trajectory: during the next sweeps site (t, i) flips iff
+        target[t, i] differs from its current field (None returns to Metropolis decisions)."""
+        if target is None:
+            lib().or_set_forced_fields(self.h, None)
+        else:
+            self._forced = np.ascontiguousarray(target, dtype=np.int32).reshape(self.nt, self.ns)
+            lib().or_set_forced_fields(self.h, _ip(self._forced))
 
     def set_thermalization(self, on):
         lib().or_set_thermalization(self.h, int(on))
