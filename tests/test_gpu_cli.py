@@ -79,3 +79,44 @@ def test_checkpoint_resume_continues_exactly(hq, tmp_path):
         b.set_rng_state(0, 0)
     a.close()
     b.close()
+
+
+def _free_port():
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _cli_rank(rank, world, port, cfg_path, outdir):
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world), RANK=str(rank),
+                      LOCAL_RANK=str(rank))
+    from __graft_entry__ import load_package
+    load_package()
+    from hubbard_b200 import cli
+    # both processes share the one GPU of this test: each runs its own chains on device 0
+    assert cli.main(["-c", cfg_path, "-o", outdir, "--device", "0"]) == 0
+
+
+def test_torchrun_mode_equals_one_process(hq, tmp_path):
+    """The command line under torchrun: two processes own chains {0, 1} and {2}, run them
+    independently and gather their bins to rank 0, which writes the reference's files. The
+    pooled bins equal those of one process running all three chains (chain c keeps seed
+    11 + c, whatever the process count)."""
+    import torch.multiprocessing as tmp
+    from hubbard_b200 import cli
+    cfg = tmp_path / "config.toml"
+    cfg.write_text(CONFIG)
+    one, two = tmp_path / "one", tmp_path / "two"
+    assert cli.main(["-c", str(cfg), "-o", str(one)]) == 0
+    tmp.start_processes(_cli_rank, args=(2, _free_port(), str(cfg), str(two)), nprocs=2, join=True,
+                        start_method="spawn")
+    for stem in ("filling", "double_occu", "swave_corr", "gf", "ldos", "spin_corr"):
+        a = (one / (stem + ".bins.out")).read_text().splitlines()
+        b = (two / (stem + ".bins.out")).read_text().splitlines()
+        assert a == b, stem
