@@ -28,7 +28,7 @@ EXPORTS = [
     "hq_upload_fields_i8", "hq_download_fields_i8", "hq_get_stream", "hq_profile_enable", "hq_profile_collect",
     "hq_equaltime_g_noalloc", "hq_autotune", "hq_get_stack", "hq_get_rng_state", "hq_set_rng_state",
 ]
-PROFILE_CLASSES = ["interval", "bchain", "udt", "gemm", "invert", "measure", "dynamic", "adjoint"]
+PROFILE_CLASSES = ["interval", "bchain", "udt", "gemm", "invert", "measure", "dynamic", "adjoint", "interval_cluster"]
 
 
 class HqChainParams(ctypes.Structure):

@@ -15,16 +15,16 @@ constexpr int kGJ = 16;  // pivot panel of the blocked Gauss-Jordan inverse
 
 // shared-memory leading dimension of an N x N matrix: odd, so that threads walking
 // consecutive columns hit distinct banks
-__host__ __device__ inline int smem_ld(int N) { return (N % 2 == 0) ? N + 1 : N; }
+__host__ __device__ constexpr inline int smem_ld(int N) { return (N % 2 == 0) ? N + 1 : N; }
 
 // leading dimension of the delayed-update panels: = 4 (mod 16) doubles, so that the DMMA
 // fragment loads of the flush are free of bank conflicts
-__host__ __device__ inline int panel_ld(int N) { return N + ((4 - N % 16) + 16) % 16; }
+__host__ __device__ constexpr inline int panel_ld(int N) { return N + ((4 - N % 16) + 16) % 16; }
 
 // leading dimension of the resident G of k_interval: = 2 (mod 8) doubles, so that the DMMA
 // accumulator tiles of the rank updates (lane 4g+q at row g, columns 2q, 2q+1) are free of
 // bank conflicts
-__host__ __device__ inline int interval_ld(int N) { return N + ((2 - N % 8) + 8) % 8; }
+__host__ __device__ constexpr inline int interval_ld(int N) { return N + ((2 - N % 8) + 8) % 8; }
 
 // bytes of dynamic shared memory of k_interval for a chain of size N with delay depth kmax
 // (matrix in smem when `resident`)
@@ -77,6 +77,88 @@ __device__ __forceinline__ void load_mat_async(double* dst, int ldd, const doubl
 }
 
 // ---------------------------------------------------------------------------------
+// ---------------------------------------------------------------------------------
+//  Bulk copies through the tensor-memory-access engine (cp.async.bulk, non-tensor form):
+//  whole matrix columns between global and shared memory, completed on an mbarrier (loads)
+//  or a bulk group (stores). Both addresses and the size must be multiples of 16 bytes:
+//  columns of an even N with an even shared leading dimension.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// waits for phase `parity` of the mbarrier with an iteration limit (each try_wait suspends for
+// a bounded time); false if the limit ran out
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+  for (int it = 0; it < (1 << 22); ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+// makes this thread's generic-proxy shared-memory writes visible to bulk copies issued later
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// whether the columns of an N x N matrix can move by bulk copies between global memory (leading
+// dimension N, 16-byte aligned base) and shared memory (leading dimension ldd, aligned base)
+__device__ __forceinline__ bool bulk_columns_ok(const double* gsrc, int N, int ldd) {
+  return (N % 2 == 0) && (ldd % 2 == 0) && ((reinterpret_cast<uintptr_t>(gsrc) & 15) == 0);
+}
+
+// Loads an N x N column-major matrix into shared memory (leading dimension ldd) by one bulk copy
+// per column, issued by warp 0 and completed on `bar` (initialised for one arrival, phase 0).
+// Every thread waits; on a wait that runs out the chain's status word is set. The caller has
+// checked bulk_columns_ok. A barrier must separate mbar_init from this call.
+__device__ __forceinline__ void load_mat_bulk(double* dst, int ldd, const double* src, int N, uint64_t* bar,
+                                              double* status) {
+  const unsigned col = static_cast<unsigned>(N) * sizeof(double);
+  if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, col * static_cast<unsigned>(N));
+  __syncwarp();
+  if (threadIdx.x < 32)
+    for (int j = threadIdx.x; j < N; j += 32) bulk_g2s(dst + (size_t)j * ldd, src + (size_t)j * N, col, bar);
+  if (!mbar_wait_bounded(bar, 0)) {
+    if (threadIdx.x == 0) *status = 1.0;
+    mbar_wait_bounded(bar, 0);  // the copies in flight still land in this CTA's shared memory
+  }
+}
+
+// Stores an N x N matrix from shared memory (leading dimension lds) to global memory (leading
+// dimension N) by one bulk copy per column from warp 0, and waits for the copies to complete.
+// Every thread calls it after its last write of the matrix.
+__device__ __forceinline__ void store_mat_bulk(double* dst, const double* src, int lds, int N) {
+  fence_proxy_async_smem();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const unsigned col = static_cast<unsigned>(N) * sizeof(double);
+    for (int j = threadIdx.x; j < N; j += 32) bulk_s2g(dst + (size_t)j * N, src + (size_t)j * lds, col);
+    bulk_commit();
+    bulk_wait_all();
+  }
+}
+
 // G[0:M, 0:Nc] += X[0:M, 0:k] Y[0:k, 0:Nc]  (X column-major ldx, Y row-major ldy, k <= 16),
 // by 16 x 32 strips of four 16 x 8 DMMA tiles that share the A fragments; the fragments of
 // all k-steps are loaded before the strip's G tiles so that their latencies overlap

@@ -10,6 +10,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -164,6 +165,7 @@ struct hq_ctx {
   std::vector<void*> extra_allocs;
   int Nmax = 0, kmax_max = 0, ntmax = 0, nstab_max = 0;
   bool resident = true;         // matrices fit in one SM's shared memory
+  bool cluster_interval = false;  // the interval kernel may run on four-CTA clusters (16 x 16 lattices)
   bool has_dynamic = false;
   // batched GEMM job lists: key (phase, dir, b) -> device pointer + count
   std::map<std::tuple<int, int, int>, std::pair<HqGemmJob*, int>> jobs;
@@ -364,7 +366,7 @@ void build_jobs(hq_ctx* c) {
 }
 
 // launch classes of the per-launch timing (hq_profile_collect)
-enum ProfClass { PC_INTERVAL = 0, PC_BCHAIN, PC_UDT, PC_GEMM, PC_INVERT, PC_MEASURE, PC_DYN, PC_ADJ, PC_COUNT };
+enum ProfClass { PC_INTERVAL = 0, PC_BCHAIN, PC_UDT, PC_GEMM, PC_INVERT, PC_MEASURE, PC_DYN, PC_ADJ, PC_INTERVAL_CL, PC_COUNT };
 
 struct ProfScope {
   hq_ctx* c;
@@ -471,6 +473,18 @@ void in_groups(hq_ctx* c, F&& body) {
   }
 }
 
+// whether the chains of the current group run their interval kernel on four-CTA clusters:
+// every one of them has the 16 x 16 lattice with the separable expK and delay depth 16
+bool interval_on_clusters(hq_ctx* c) {
+  if (!c->cluster_interval) return false;
+  const int c0 = c->cur_st ? c->cur_c0 : 0, n = c->cur_st ? c->cur_n : c->n;
+  for (int i = c0; i < c0 + n; ++i) {
+    const HqChain& d = c->desc[i];
+    if (!hq::interval_cluster_ok(d.N, d.L, d.expk_mode, d.kmax)) return false;
+  }
+  return true;
+}
+
 void issue_sweep(hq_ctx* c, int dir, int flags) {
   c->prof_next = 0;
   const int kf = flags & (HQ_F_MEASURE | HQ_F_SNAPSHOT | HQ_F_LOG_RATIOS);
@@ -478,7 +492,13 @@ void issue_sweep(hq_ctx* c, int dir, int flags) {
     in_groups(c, [&] {
       const Cur gr = cur(c);
       for (int b = 0; b < c->nstab_max; ++b) {
-        { ProfScope ps(c, PC_INTERVAL); HQ_CUDA(hq::launch_interval(gr.d, gr.n, dir, b, kf, c->Nmax, c->kmax_max, c->resident, gr.st)); }
+        if (interval_on_clusters(c)) {
+          ProfScope ps(c, PC_INTERVAL_CL);
+          HQ_CUDA(hq::launch_interval_cl(gr.d, gr.n, dir, b, kf, gr.st));
+        } else {
+          ProfScope ps(c, PC_INTERVAL);
+          HQ_CUDA(hq::launch_interval(gr.d, gr.n, dir, b, kf, c->Nmax, c->kmax_max, c->resident, gr.st));
+        }
         push_step(c, dir, dir, b);
         builder_equaltime(c, dir, b);
         if (kf & (HQ_F_MEASURE | HQ_F_SNAPSHOT)) { ProfScope ps(c, PC_MEASURE); HQ_CUDA(hq::launch_measure(gr.d, gr.n, dir, b, kf, gr.st)); }
@@ -723,6 +743,18 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   }
   c->desc.shrink_to_fit();
   HQ_CUDA(hq::prepare_kernels(c->Nmax, c->kmax_max, c->resident));
+  // chains too large for one SM: the interval kernel of 16 x 16 lattices runs on four-CTA
+  // clusters with G in their distributed shared memory (HQ_INTERVAL_CLUSTER=0 keeps the
+  // global-memory path, for comparisons)
+  if (!c->resident) {
+    const char* env = std::getenv("HQ_INTERVAL_CLUSTER");
+    bool any = false;
+    for (int i = 0; i < n_chains; ++i) any = any || (c->ch[i].N == 256 && c->ch[i].p.nl == 16);
+    if (any && !(env && std::strcmp(env, "0") == 0)) {
+      HQ_CUDA(hq::prepare_interval_cl());
+      c->cluster_interval = hq::interval_cl_max_clusters() > 0;
+    }
+  }
   HQ_CUDA(cudaMalloc(&c->d_desc, c->desc.size() * sizeof(HqChain)));
   // the gather buffers of hq_get_estimators_all, so that no read allocates
   HQ_CUDA(cudaMalloc(&c->d_acc_all, size_t(c->n) * HQ_ACC_COUNT * sizeof(double)));

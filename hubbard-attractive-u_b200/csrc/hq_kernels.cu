@@ -388,7 +388,7 @@ size_t smem_matrix_bytes(int Nmax, bool resident, int extra_doubles) {
 // context of small chains never lowers the limit an existing context of larger chains
 // launches with.
 constexpr int kMaxTrackedDevices = 64;
-constexpr int kTrackedKernels = 6;
+constexpr int kTrackedKernels = 7;
 static size_t g_smem_set[kMaxTrackedDevices][kTrackedKernels];
 
 static cudaError_t raise_smem(int slot, const void* fn, size_t bytes) {
@@ -426,6 +426,8 @@ cudaError_t prepare_kernels(int Nmax, int kmax, bool resident) {
   if ((e = raise_smem(5, (const void*)k_adj_interval, mat_stage)) != cudaSuccess) return e;
   return cudaSuccess;
 }
+
+cudaError_t prepare_interval_cl() { return raise_smem(6, fn_interval_cl(), smem_interval_cl_bytes()); }
 
 cudaError_t launch_bchain(const HqChain* chains, int n, int dir, int b, int Nmax, bool resident, cudaStream_t st) {
   const size_t bytes = smem_matrix_bytes(Nmax, resident, 8 * (((Nmax + 15) & ~15) + 4) + 64);

@@ -29,6 +29,14 @@ cudaError_t launch_gather_acc(const HqChain* chains, int n, double* out, cudaStr
 const void* fn_interval();
 const void* fn_udt();
 const void* fn_invert();
+// the interval kernel on a four-CTA cluster per chain (16 x 16 lattice, separable expK, delay
+// depth 16): G spread over the cluster's shared memory
+bool interval_cluster_ok(int N, int L, int expk_mode, int kmax);
+size_t smem_interval_cl_bytes();
+cudaError_t launch_interval_cl(const HqChain* chains, int n, int dir, int b, int flags, cudaStream_t st);
+const void* fn_interval_cl();
+int interval_cl_max_clusters();
+cudaError_t prepare_interval_cl();
 cudaError_t launch_adj_interval(const HqChain* chains, int n, int b, int Nmax, bool resident, cudaStream_t st);
 cudaError_t launch_adj_last(const HqChain* chains, int n, int b, cudaStream_t st);
 }  // namespace hq

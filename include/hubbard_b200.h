@@ -166,7 +166,8 @@ HQ_API int hq_get_stream(hq_ctx* ctx, void** stream);
  * captured graphs). hq_profile_collect waits for the stream and adds the elapsed time of
  * every launch of the most recent sweep to ms[class] and 1 to counts[class]. Classes:
  * 0 interval (wrap + Metropolis), 1 B chain, 2 UDV factorisation, 3 batched GEMM,
- * 4 inversion, 5 boundary measurement, 6 displaced propagation, 7 log-det adjoint. */
+ * 4 inversion, 5 boundary measurement, 6 displaced propagation, 7 log-det adjoint,
+ * 8 interval on four-CTA clusters (16 x 16 lattices, G in distributed shared memory). */
 HQ_API int hq_profile_enable(hq_ctx* ctx, int on);
 HQ_API int hq_profile_collect(hq_ctx* ctx, double* ms, long long* counts, int nclasses);
 

@@ -345,3 +345,56 @@ def test_profiling_with_and_without_graphs(hq):
         i = classes.index("interval")
         assert cnt[i] == 4 and ms[i] > 0.0, (use_graph, cnt, ms)
     e.close()
+
+
+def test_c5_cluster_path_equals_global_memory_path(hq, oracle):
+    """16x16: the interval kernel on four-CTA clusters (G in the cluster's distributed shared
+    memory) against the one-CTA kernel with G in global memory (HQ_INTERVAL_CLUSTER=0): the
+    same fields, counts and G (each element sees the same floating-point operations), and the
+    oracle's fields. 8 chains, beta = 1.6 (32 slices, pace 8), snapshots and ratio log on."""
+    import os
+    cfgs = [dict(nl=16, u=4.0, mu=-0.2, beta=1.6, nt=32, stabilization_pace=8, seed=5000 + c, expk_mode=1,
+                 snapshots=1) for c in range(8)]
+    engines = []
+    for cluster in (True, False):
+        if not cluster:
+            os.environ["HQ_INTERVAL_CLUSTER"] = "0"
+        try:
+            e = hq.Engine(cfgs)
+        finally:
+            os.environ.pop("HQ_INTERVAL_CLUSTER", None)
+        e.fields_random()
+        e.init()
+        e.ratio_log(0, capacity=4 * 32 * 256)
+        e.profile_enable(True)
+        engines.append(e)
+    classes = hq.capi.PROFILE_CLASSES
+    o = oracle.OracleChain(16, u=4.0, mu=-0.2, beta=1.6, nt=32, pace=8, seed=5000)
+    o.fields_random()
+    o.init()
+    a, b = engines
+    for d in (UP, DOWN, UP, DOWN):
+        counts = []
+        for e in engines:
+            ms = np.zeros(len(classes))
+            cnt = np.zeros(len(classes), dtype=np.int64)
+            e.sweep(d, hq.SWEEP_MEASURE | hq.SWEEP_SNAPSHOT | hq.SWEEP_LOG_RATIOS)
+            e.profile_collect(ms, cnt)
+            counts.append(cnt)
+        o.sweep(d)
+        assert counts[0][classes.index("interval_cluster")] == 4 and counts[0][classes.index("interval")] == 0
+        assert counts[1][classes.index("interval")] == 4 and counts[1][classes.index("interval_cluster")] == 0
+        assert np.array_equal(a.fields(0), o.fields())
+        for c in range(8):
+            assert np.array_equal(a.fields(c), b.fields(c)), c
+            assert np.abs(a.g(c) - b.g(c)).max() <= 1e-13, (c, np.abs(a.g(c) - b.g(c)).max())
+            for t in range(0, 32, 5):
+                assert np.abs(a.g(c, hq.G_TT, t) - b.g(c, hq.G_TT, t)).max() <= 1e-13, (c, t)
+        ea, eb = a.estimators_all(), b.estimators_all()
+        assert np.array_equal(ea[:, 3:], eb[:, 3:])
+        assert np.abs(ea[:, :3] - eb[:, :3]).max() <= 1e-12 * np.abs(eb[:, :3]).max()
+    assert np.array_equal(a.ratio_log(0), b.ratio_log(0))
+    g = o.g()
+    assert np.abs(a.g(0) - g).max() <= 1e-10 * max(1.0, np.abs(g).max())
+    for e in engines:
+        e.close()
