@@ -27,13 +27,18 @@ __device__ __forceinline__ void metropolis_slice_blk(const HqChain& ch, double* 
   double acc_count = 0.0;
   for (int b0 = 0, bi = 0; b0 < N; b0 += NB, ++bi) {
     if (warp == 0) {
-      if constexpr (NB == 16) walk_block16(ch, G, ld, sh, b0, min(NB, N - b0), log, bi & 1, acc_count);
-      else walk_block<NB>(ch, G, ld, sh, b0, min(NB, N - b0), log, bi & 1, acc_count);
+      const int nb = min(NB, N - b0);
+      if constexpr (NB == 16) {
+        if (walk_block16<false>(ch, G, ld, sh, b0, nb, log, bi & 1)) walk_block16<true>(ch, G, ld, sh, b0, nb, log, bi & 1);
+      } else {
+        if (walk_block<NB, false>(ch, G, ld, sh, b0, nb, log, bi & 1)) walk_block<NB, true>(ch, G, ld, sh, b0, nb, log, bi & 1);
+      }
     }
     __syncthreads();
     // the count alternates between two words: with no flush (a == 0) no barrier follows,
     // and warp 0 writes the next block's count while other warps may still read this one
     const int a = sh.ired[bi & 1];
+    if (tid == 0) acc_count += a;
     if (a == 0) continue;
     build_panels<NB>(G, ld, N, sh, ldp, a, b0);
     __syncthreads();

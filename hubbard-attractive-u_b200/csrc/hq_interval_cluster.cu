@@ -195,10 +195,13 @@ __device__ __forceinline__ void cl_metropolis(const HqChain& ch, double* Gc, int
   for (int b0 = 0, bi = 0; b0 < kN; b0 += 16, ++bi) {
     const int owner = b0 / kNC;
     const int slot = bi & 1;
-    if (rank == owner && warp == 0) walk_block16(ch, Gs, kLd, sh, b0, 16, log, slot, acc_count);
+    if (rank == owner && warp == 0) {
+      if (walk_block16<false>(ch, Gs, kLd, sh, b0, 16, log, slot)) walk_block16<true>(ch, Gs, kLd, sh, b0, 16, log, slot);
+    }
     cluster.sync();  // the walk's records are visible to the cluster
     const int* o_ired = cluster.map_shared_rank(sh.ired, owner);
     const int a = o_ired[slot];
+    if (rank == owner && tid == 0) acc_count += a;
     if (a == 0) continue;
     if (rank != owner) {
       const double* oxt = cluster.map_shared_rank(sh.xt, owner);

