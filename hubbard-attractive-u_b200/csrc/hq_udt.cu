@@ -251,9 +251,11 @@ __device__ void wy_apply(double* A, int ld, int N, int p0, const double* Vb, int
 }
 
 // Panel-wise column pivoting before the panel [p0, p1): the norms of the trailing columns over
-// rows p0..N-1 (the matrix as updated by the earlier panels), then p1 - p0 selection steps,
-// each swapping the remaining column of largest norm (smallest index among equal norms) into
-// the next panel position; whole columns move, with their norm and their original index.
+// rows p0..N-1 (the matrix as updated by the earlier panels); warp 0 then makes the p1 - p0
+// selections one after the other, each moving the remaining column of largest norm (smallest
+// index among equal norms) into the next panel position (norms and original indices swap with
+// it), and records the swaps; finally every thread applies the recorded swaps, in order, to
+// the rows it owns. piv holds kQB ints.
 __device__ void panel_pivot(double* A, int ld, int N, int p0, int p1, double* nrm, int* order, int* piv) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (int j = p0 + warp; j < N; j += nwarps) {
@@ -266,8 +268,8 @@ __device__ void panel_pivot(double* A, int ld, int N, int p0, int p1, double* nr
     if (lane == 0) nrm[j] = s2;
   }
   __syncthreads();
-  for (int q = p0; q < p1; ++q) {
-    if (warp == 0) {
+  if (warp == 0) {
+    for (int q = p0; q < p1; ++q) {
       double best = -1.0;
       int bj = N;
       for (int j = q + lane; j < N; j += 32) {
@@ -280,23 +282,28 @@ __device__ void panel_pivot(double* A, int ld, int N, int p0, int p1, double* nr
         const int oj = __shfl_xor_sync(0xffffffffu, bj, o);
         if (ob > best || (ob == best && oj < bj)) { best = ob; bj = oj; }
       }
-      if (lane == 0) *piv = bj;
+      if (bj >= N) bj = q;
+      if (lane == 0) {
+        piv[q - p0] = bj;
+        if (bj != q) {
+          const double tn = nrm[q]; nrm[q] = nrm[bj]; nrm[bj] = tn;
+          const int to = order[q]; order[q] = order[bj]; order[bj] = to;
+        }
+      }
+      __syncwarp();
     }
-    __syncthreads();
-    const int jp = *piv;
-    if (jp != q && jp < N) {
-      for (int r = threadIdx.x; r < N; r += blockDim.x) {
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < N; r += blockDim.x)
+    for (int q = p0; q < p1; ++q) {
+      const int jp = piv[q - p0];
+      if (jp != q) {
         const double t0 = A[r + (size_t)q * ld];
         A[r + (size_t)q * ld] = A[r + (size_t)jp * ld];
         A[r + (size_t)jp * ld] = t0;
       }
-      if (threadIdx.x == 0) {
-        const double tn = nrm[q]; nrm[q] = nrm[jp]; nrm[jp] = tn;
-        const int to = order[q]; order[q] = order[jp]; order[jp] = to;
-      }
     }
-    __syncthreads();
-  }
+  __syncthreads();
 }
 
 __global__ void __launch_bounds__(HQ_THREADS, 1)
@@ -352,10 +359,10 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
   }
   __syncthreads();
   // ---- blocked Householder QR ----
-  __shared__ int piv;
+  __shared__ int piv[kQB];
   for (int p0 = 0; p0 < N; p0 += kQB) {
     const int p1 = min(p0 + kQB, N);
-    if (p0 > 0) panel_pivot(A, ld, N, p0, p1, nrm, order, &piv);
+    if (p0 > 0) panel_pivot(A, ld, N, p0, p1, nrm, order, piv);
     if (N <= 160) qr_panel_reg<5>(A, ld, N, p0, p1, tau);
     else qr_panel(A, ld, N, p0, p1, tau);
     if (p1 < N) {
