@@ -428,10 +428,27 @@ void upload_desc(hq_ctx* c) {
   HQ_CUDA(cudaMemcpy(c->d_desc, c->desc.data(), c->desc.size() * sizeof(HqChain), cudaMemcpyHostToDevice));
 }
 
+// whether the chains of the current group run their interval kernel on four-CTA clusters (and
+// their B chain on four column blocks): every one of them has the 16 x 16 lattice with the
+// separable expK and delay depth 16
+bool interval_on_clusters(hq_ctx* c) {
+  if (!c->cluster_interval) return false;
+  const int c0 = c->cur_st ? c->cur_c0 : 0, n = c->cur_st ? c->cur_n : c->n;
+  for (int i = c0; i < c0 + n; ++i) {
+    const HqChain& d = c->desc[i];
+    if (!hq::interval_cluster_ok(d.N, d.L, d.expk_mode, d.kmax)) return false;
+  }
+  return true;
+}
+
 // one stack push of interval b: bchain -> UDV -> cumulative Vt
 void push_step(hq_ctx* c, int dir_kernel, int dir_jobs, int b) {
   const Cur g = cur(c);
-  { ProfScope ps(c, PC_BCHAIN); HQ_CUDA(hq::launch_bchain(g.d, g.n, dir_kernel, b, c->Nmax, c->resident, g.st)); }
+  {
+    ProfScope ps(c, PC_BCHAIN);
+    if (interval_on_clusters(c)) HQ_CUDA(hq::launch_bchain_cols(g.d, g.n, dir_kernel, b, g.st));
+    else HQ_CUDA(hq::launch_bchain(g.d, g.n, dir_kernel, b, c->Nmax, c->resident, g.st));
+  }
   const int side = (dir_kernel == HQ_DOWN) ? 1 : 0;
   { ProfScope ps(c, PC_UDT); HQ_CUDA(hq::launch_udt(g.d, g.n, side, b, c->Nmax, c->resident, g.st)); }
   run_jobs(c, PH_PUSH, dir_jobs, b);
@@ -471,18 +488,6 @@ void in_groups(hq_ctx* c, F&& body) {
       HQ_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join[g], 0));
     }
   }
-}
-
-// whether the chains of the current group run their interval kernel on four-CTA clusters:
-// every one of them has the 16 x 16 lattice with the separable expK and delay depth 16
-bool interval_on_clusters(hq_ctx* c) {
-  if (!c->cluster_interval) return false;
-  const int c0 = c->cur_st ? c->cur_c0 : 0, n = c->cur_st ? c->cur_n : c->n;
-  for (int i = c0; i < c0 + n; ++i) {
-    const HqChain& d = c->desc[i];
-    if (!hq::interval_cluster_ok(d.N, d.L, d.expk_mode, d.kmax)) return false;
-  }
-  return true;
 }
 
 void issue_sweep(hq_ctx* c, int dir, int flags) {

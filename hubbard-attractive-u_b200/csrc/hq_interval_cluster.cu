@@ -421,6 +421,76 @@ k_interval_cl(const HqChain* __restrict__ chains, int nchains, int dir, int b, i
   cluster.sync();  // no CTA leaves while another may still read its shared memory
 }
 
+// ---------------------------------------------------------------------------------
+//  k_bchain_cols: the B-matrix chain of one interval for the 16 x 16 lattice (the role of
+//  k_bchain, src/dqmc_core.cpp:190, :251 with the (M U) S product of svd_stack.hpp:144).
+//  X <- B(t)...(U_top D_top) acts on every column of X on its own, so four CTAs per chain each
+//  take 64 columns into shared memory; the one-CTA kernel would keep the 512 KB X in global
+//  memory at this size. Same separable passes and arithmetic as k_bchain.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(HQ_INT_THREADS, 1)
+k_bchain_cols(const HqChain* __restrict__ chains, int nchains, int dir, int b) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ HqChain ch;
+  __shared__ int8_t s[kN];
+  const int c = blockIdx.x / kCl, q = blockIdx.x % kCl;  // chain, column block
+  if (c >= nchains) return;
+  if (threadIdx.x == 0) ch = chains[c];
+  __syncthreads();
+  if (!ch.active || b >= ch.n_stab) return;
+  int t_lo, t_hi;
+  interval_range(ch.nt, ch.pace, ch.n_stab, dir, b, t_lo, t_hi);
+  const int side = (dir == HQ_DOWN) ? 1 : 0;
+  const int top = b - 1;  // the pushing stack holds b entries before this push
+  const int c0 = q * kNC;
+  const size_t NN = (size_t)kN * kN;
+  double* Xc = smem;                      // kN x kNC, leading dimension kLd
+  double* Dc = smem + (size_t)kNC * kLd;  // D of the stack top at the block's columns
+  if (top >= 0) {
+    const double* U = ch.stackU + ((size_t)side * ch.n_stab + top) * NN;
+    const double* D = ch.stackD + ((size_t)side * ch.n_stab + top) * kN;
+    for (int k = threadIdx.x; k < kNC; k += blockDim.x) cp_async_8(Dc + k, D + c0 + k, true);
+    for (int j = threadIdx.x >> 5; j < kNC; j += blockDim.x >> 5)
+      for (int i = threadIdx.x & 31; i < kN; i += 32) cp_async_8(Xc + i + (size_t)j * kLd, U + i + (size_t)(c0 + j) * kN, true);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    for (int j = threadIdx.x >> 5; j < kNC; j += blockDim.x >> 5)
+      for (int i = threadIdx.x & 31; i < kN; i += 32) Xc[i + (size_t)j * kLd] *= Dc[j];
+  } else {
+    for (int j = threadIdx.x >> 5; j < kNC; j += blockDim.x >> 5)
+      for (int i = threadIdx.x & 31; i < kN; i += 32) Xc[i + (size_t)j * kLd] = (i == c0 + j ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  const int nsl = t_hi - t_lo + 1;
+  for (int step = 0; step < nsl; ++step) {
+    const int t = (dir == HQ_DOWN) ? (t_hi - step) : (t_lo + step);
+    const int l = t % ch.nt;
+    for (int i = threadIdx.x; i < kN; i += blockDim.x) s[i] = ch.fields[(size_t)l * kN + i];
+    __syncthreads();
+    // e^{V} rides on the first pass (down: B^T = E e^V) or the last pass (up: B = e^V E)
+    if (dir == HQ_DOWN) {
+      cl_local_pass<0, 0, 1>(Xc, c0, ch.sep_a, ch.sep_c, s, ch.ev_p, ch.ev_m, 1.0, 1.0);
+      __syncthreads();
+      cl_local_pass<0, 1, 0>(Xc, c0, ch.sep_a, ch.sep_c, s, 1.0, 1.0, 1.0, 1.0);
+    } else {
+      cl_local_pass<0, 0, 0>(Xc, c0, ch.sep_a, ch.sep_c, s, 1.0, 1.0, 1.0, 1.0);
+      __syncthreads();
+      cl_local_pass<0, 1, 2>(Xc, c0, ch.sep_a, ch.sep_c, s, ch.ev_p, ch.ev_m, 1.0, 1.0);
+    }
+    __syncthreads();
+  }
+  for (int j = threadIdx.x >> 5; j < kNC; j += blockDim.x >> 5)
+    for (int i = threadIdx.x & 31; i < kN; i += 32) ch.X[i + (size_t)(c0 + j) * kN] = Xc[i + (size_t)j * kLd];
+}
+
+size_t smem_bchain_cols_bytes() { return ((size_t)kNC * kLd + kNC) * sizeof(double); }
+cudaError_t launch_bchain_cols(const HqChain* chains, int n, int dir, int b, cudaStream_t st) {
+  k_bchain_cols<<<n * kCl, HQ_INT_THREADS, smem_bchain_cols_bytes(), st>>>(chains, n, dir, b);
+  return cudaGetLastError();
+}
+const void* fn_bchain_cols() { return (const void*)k_bchain_cols; }
+
 cudaError_t launch_interval_cl(const HqChain* chains, int n, int dir, int b, int flags, cudaStream_t st) {
   k_interval_cl<<<n * kCl, HQ_INT_THREADS, smem_interval_cl_bytes(), st>>>(chains, n, dir, b, flags);
   return cudaGetLastError();

@@ -388,7 +388,7 @@ size_t smem_matrix_bytes(int Nmax, bool resident, int extra_doubles) {
 // context of small chains never lowers the limit an existing context of larger chains
 // launches with.
 constexpr int kMaxTrackedDevices = 64;
-constexpr int kTrackedKernels = 7;
+constexpr int kTrackedKernels = 8;
 static size_t g_smem_set[kMaxTrackedDevices][kTrackedKernels];
 
 static cudaError_t raise_smem(int slot, const void* fn, size_t bytes) {
@@ -427,7 +427,11 @@ cudaError_t prepare_kernels(int Nmax, int kmax, bool resident) {
   return cudaSuccess;
 }
 
-cudaError_t prepare_interval_cl() { return raise_smem(6, fn_interval_cl(), smem_interval_cl_bytes()); }
+cudaError_t prepare_interval_cl() {
+  const cudaError_t e = raise_smem(6, fn_interval_cl(), smem_interval_cl_bytes());
+  if (e != cudaSuccess) return e;
+  return raise_smem(7, fn_bchain_cols(), smem_bchain_cols_bytes());
+}
 
 cudaError_t launch_bchain(const HqChain* chains, int n, int dir, int b, int Nmax, bool resident, cudaStream_t st) {
   const size_t bytes = smem_matrix_bytes(Nmax, resident, 8 * (((Nmax + 15) & ~15) + 4) + 64);

@@ -37,6 +37,10 @@ cudaError_t launch_interval_cl(const HqChain* chains, int n, int dir, int b, int
 const void* fn_interval_cl();
 int interval_cl_max_clusters();
 cudaError_t prepare_interval_cl();
+// the B chain of the 16 x 16 lattice split over four CTAs per chain by column blocks
+size_t smem_bchain_cols_bytes();
+cudaError_t launch_bchain_cols(const HqChain* chains, int n, int dir, int b, cudaStream_t st);
+const void* fn_bchain_cols();
 cudaError_t launch_adj_interval(const HqChain* chains, int n, int b, int Nmax, bool resident, cudaStream_t st);
 cudaError_t launch_adj_last(const HqChain* chains, int n, int b, cudaStream_t st);
 }  // namespace hq
