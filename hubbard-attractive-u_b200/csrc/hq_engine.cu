@@ -182,10 +182,12 @@ struct hq_ctx {
   size_t prof_next = 0;
   // chain groups of the up / down sweeps: each group's kernels run on its own stream, so that
   // one group's launches fill the SMs left idle by the other's last wave
-  static constexpr int kGroups = 2;
+  // (two groups when every chain is resident in one SM's shared memory and the groups fill the
+  // GPU; four for larger chains, whose per-chain phases leave most SMs idle on their own)
+  static constexpr int kGroups = 4;
   int ngroups = 1;
-  cudaStream_t gstream[kGroups] = {nullptr, nullptr};
-  cudaEvent_t ev_fork = nullptr, ev_join[kGroups] = {nullptr, nullptr};
+  cudaStream_t gstream[kGroups] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[kGroups] = {nullptr, nullptr, nullptr, nullptr};
   // the chains and stream the launch helpers currently issue for (default: all, main stream)
   int cur_c0 = 0, cur_n = 0;
   cudaStream_t cur_st = nullptr;
@@ -568,13 +570,6 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   c->device = device;
   HQ_CUDA(cudaSetDevice(device));
   HQ_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-  if (n_chains >= 32) {
-    c->ngroups = hq_ctx::kGroups;
-    c->gstream[0] = c->stream;
-    for (int g = 1; g < c->ngroups; ++g) HQ_CUDA(cudaStreamCreateWithFlags(&c->gstream[g], cudaStreamNonBlocking));
-    HQ_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
-    for (int g = 0; g < c->ngroups; ++g) HQ_CUDA(cudaEventCreateWithFlags(&c->ev_join[g], cudaEventDisableTiming));
-  }
   c->n = n_chains;
   c->ch.resize(n_chains);
   c->desc.resize(n_chains);
@@ -620,6 +615,15 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   }
   if (hq::smem_interval_bytes(c->Nmax, c->kmax_max, c->resident) > budget)
     throw HqError(HQ_E_INVALID, "delay depth does not fit in shared memory");
+  // chain groups on forked streams (see in_groups)
+  if (n_chains >= 32) {
+    c->ngroups = c->resident ? 2 : hq_ctx::kGroups;
+    if (n_chains < 16 * c->ngroups) c->ngroups = 2;
+    c->gstream[0] = c->stream;
+    for (int g = 1; g < c->ngroups; ++g) HQ_CUDA(cudaStreamCreateWithFlags(&c->gstream[g], cudaStreamNonBlocking));
+    HQ_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    for (int g = 0; g < c->ngroups; ++g) HQ_CUDA(cudaEventCreateWithFlags(&c->ev_join[g], cudaEventDisableTiming));
+  }
   // ---- arena layout ----
   struct Off { size_t G, Gt0, G0t, fields, rng, X, sU, sD, sVt, W[6], stt, st0, s0t, acc, dyn, rcount; };
   std::vector<Off> offs(n_chains);
