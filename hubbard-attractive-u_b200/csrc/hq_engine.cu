@@ -182,9 +182,8 @@ struct hq_ctx {
   size_t prof_next = 0;
   // chain groups of the up / down sweeps: each group's kernels run on its own stream, so that
   // one group's launches fill the SMs left idle by the other's last wave
-  // (two groups when the chains are alike and resident in one SM's shared memory, so that the
-  // groups fill the GPU; four for larger chains, whose per-chain phases leave most SMs idle on
-  // their own, and for uneven chains, whose launches wait for their slowest chain)
+  // (two groups when the chains are resident in one SM's shared memory, so that the groups fill
+  // the GPU; four for larger chains, whose per-chain phases leave most SMs idle on their own)
   static constexpr int kGroups = 4;
   int ngroups = 1;
   cudaStream_t gstream[kGroups] = {nullptr, nullptr, nullptr, nullptr};
@@ -618,10 +617,7 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
     throw HqError(HQ_E_INVALID, "delay depth does not fit in shared memory");
   // chain groups on forked streams (see in_groups)
   if (n_chains >= 32) {
-    bool uneven = false;
-    for (int i = 1; i < n_chains; ++i)
-      uneven = uneven || c->ch[i].N != c->ch[0].N || c->ch[i].n_stab != c->ch[0].n_stab;
-    c->ngroups = (c->resident && !uneven) ? 2 : hq_ctx::kGroups;
+    c->ngroups = c->resident ? 2 : hq_ctx::kGroups;
     if (n_chains < 16 * c->ngroups) c->ngroups = 2;
     c->gstream[0] = c->stream;
     for (int g = 1; g < c->ngroups; ++g) HQ_CUDA(cudaStreamCreateWithFlags(&c->gstream[g], cudaStreamNonBlocking));
