@@ -460,8 +460,8 @@ def run_gpu(args):
                        "delay_depth": depths[0] if len(depths) == 1 else depths, "cuda_graph": True,
                        "thermalization_sweeps": args.thermalize,
                        "autotune": [{"nl": t["nl"], "expk": "separable" if t["expk_mode"] == 1 else "dense",
-                                     "k": t["delay_depth"], "ms_per_sweep": round(t["ms_per_sweep"], 3),
-                                     "chosen": t["chosen"]} for t in tune],
+                                     "k": t["delay_depth"], "cluster": t["cluster_size"],
+                                     "ms_per_sweep": round(t["ms_per_sweep"], 3), "chosen": t["chosen"]} for t in tune],
                        "l2": "working set per GPU of chain state far above the 126 MB L2 (no flush needed)"})
         line = {
             "metric": METRIC if metric_wl else f"sweeps/s ({args.workload})", "value": value, "unit": "sweeps/s",

@@ -55,6 +55,7 @@ class HqTuneEntry(ctypes.Structure):
         ("delay_depth", ctypes.c_int),
         ("ms_per_sweep", ctypes.c_double),
         ("chosen", ctypes.c_int),
+        ("cluster_size", ctypes.c_int),
     ]
 
 
@@ -272,7 +273,7 @@ class Engine:
         n = ctypes.c_int(0)
         check(lib().hq_autotune(self.h, int(sweeps), buf, cap, ctypes.byref(n)))
         return [dict(nl=e.nl, expk_mode=e.expk_mode, delay_depth=e.delay_depth, ms_per_sweep=e.ms_per_sweep,
-                     chosen=bool(e.chosen)) for e in buf[:min(n.value, cap)]]
+                     chosen=bool(e.chosen), cluster_size=e.cluster_size) for e in buf[:min(n.value, cap)]]
 
     def stack(self, chain, side):
         """(length, U, D, V) of the top of a chain's left (0) or right (1) UDV stack; the

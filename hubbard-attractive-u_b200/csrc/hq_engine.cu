@@ -166,6 +166,7 @@ struct hq_ctx {
   int Nmax = 0, kmax_max = 0, ntmax = 0, nstab_max = 0;
   bool resident = true;         // matrices fit in one SM's shared memory
   bool cluster_interval = false;  // the interval kernel may run on four-CTA clusters (16 x 16 lattices)
+  bool cluster_capable = false;   // the device can run them (the autotuner may switch them off)
   bool has_dynamic = false;
   // batched GEMM job lists: key (phase, dir, b) -> device pointer + count
   std::map<std::tuple<int, int, int>, std::pair<HqGemmJob*, int>> jobs;
@@ -761,7 +762,8 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
     for (int i = 0; i < n_chains; ++i) any = any || (c->ch[i].N == 256 && c->ch[i].p.nl == 16);
     if (any && !(env && std::strcmp(env, "0") == 0)) {
       HQ_CUDA(hq::prepare_interval_cl());
-      c->cluster_interval = hq::interval_cl_max_clusters() > 0;
+      c->cluster_capable = hq::interval_cl_max_clusters() > 0;
+      c->cluster_interval = c->cluster_capable;
     }
   }
   HQ_CUDA(cudaMalloc(&c->d_desc, c->desc.size() * sizeof(HqChain)));
@@ -1253,10 +1255,17 @@ int hq_autotune(hq_ctx* c, int sweeps, hq_tune_entry* entries, int capacity, int
       std::vector<int> depths;
       for (int k : {4, 8, 16})
         if (k <= c->kmax_max) depths.push_back(k);
+      // cluster sizes: four CTAs per chain (G in distributed shared memory) where the lattice
+      // allows it, one CTA with G in global memory otherwise
+      std::vector<int> clusters{1};
+      if (c->cluster_capable && hq::interval_cluster_ok(nl * nl, nl, HQ_EXPK_SEPARABLE, 16)) clusters = {4, 1};
       double best = 1e300;
       size_t best_at = out.size();
+      for (int cl : clusters)
       for (int mode : modes)
         for (int k : depths) {
+          if (cl == 4 && !hq::interval_cluster_ok(nl * nl, nl, mode, k)) continue;
+          c->cluster_interval = (cl == 4);
           for (int i : g.second) { c->desc[i].expk_mode = mode; c->desc[i].kmax = k; }
           upload_desc(c);
           run(1);  // warm-up
@@ -1269,10 +1278,12 @@ int hq_autotune(hq_ctx* c, int sweeps, hq_tune_entry* entries, int capacity, int
           restore();
           hq_tune_entry t;
           t.nl = nl; t.expk_mode = mode; t.delay_depth = k; t.ms_per_sweep = double(ms) / sweeps; t.chosen = 0;
+          t.cluster_size = cl;
           if (t.ms_per_sweep < best) { best = t.ms_per_sweep; best_at = out.size(); }
           out.push_back(t);
         }
       out[best_at].chosen = 1;
+      c->cluster_interval = c->cluster_capable && out[best_at].cluster_size == 4;
       for (int i : g.second) {
         c->desc[i].expk_mode = out[best_at].expk_mode;
         c->desc[i].kmax = out[best_at].delay_depth;
@@ -1282,6 +1293,9 @@ int hq_autotune(hq_ctx* c, int sweeps, hq_tune_entry* entries, int capacity, int
     }
     upload_desc(c);
     HQ_CUDA(cudaStreamSynchronize(c->stream));
+    // captured sweeps hold the kernel choice of their capture
+    for (auto& gr : c->graphs) cudaGraphExecDestroy(gr.second);
+    c->graphs.clear();
   } catch (...) {
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);

@@ -196,14 +196,17 @@ typedef struct {
   int delay_depth;     /* sites per submatrix-update block */
   double ms_per_sweep; /* device time of one directional sweep of the whole context */
   int chosen;          /* 1: the candidate now in use for this lattice size */
+  int cluster_size;    /* CTAs per chain of the interval kernel: 4 (G in a cluster's shared memory) or 1 */
 } hq_tune_entry;
 
 /* Picks, per lattice size, the expK application (the is_fft choice of the reference's
- * config, src/hubbard.cpp:38-80, here separable circulant passes vs dense DMMA GEMM) and
- * the delay depth by timing `sweeps` directional sweeps of the whole context per candidate.
- * The device state is restored after each candidate: the Markov chains are unaffected.
- * Needs hq_init_stacks_and_g; allocates one temporary copy of the context's device state.
- * Writes up to `capacity` entries and the total count to *n_entries. */
+ * config, src/hubbard.cpp:38-80, here separable circulant passes vs dense DMMA GEMM), the
+ * delay depth and, for the 16 x 16 lattice, the cluster size of the interval kernel (four
+ * CTAs with G in distributed shared memory, or one CTA with G in global memory) by timing
+ * `sweeps` directional sweeps of the whole context per candidate. The device state is
+ * restored after each candidate: the Markov chains are unaffected. Captured sweep graphs are
+ * dropped (recapture them). Needs hq_init_stacks_and_g; allocates one temporary copy of the
+ * context's device state. Writes up to `capacity` entries and the total count to *n_entries. */
 HQ_API int hq_autotune(hq_ctx* ctx, int sweeps, hq_tune_entry* entries, int capacity, int* n_entries);
 
 /* Host <-> device copy of the raw device state of all chains' fields (int8, [chain][nt][N])

@@ -49,3 +49,29 @@ def test_autotune_needs_initialised_stacks(hq):
     with pytest.raises(hq.HqError):
         e.autotune(sweeps=0)
     e.close()
+
+
+def test_autotune_chooses_the_cluster_size_of_16x16_chains(hq):
+    """16 x 16 lattice: the candidates add the interval kernel on four-CTA clusters (separable
+    expK, delay depth 16) to the one-CTA ones; the chosen one is the fastest and the chains
+    continue exactly as an untuned context (both paths give the same arithmetic)."""
+    cfg = [dict(nl=16, u=4.0, mu=-0.2, beta=0.8, nt=16, stabilization_pace=8, seed=5000 + c) for c in range(4)]
+    a, b = hq.Engine(cfg), hq.Engine(cfg)
+    for x in (a, b):
+        x.fields_random()
+        x.init()
+    table = a.autotune(sweeps=1)
+    clustered = [t for t in table if t["cluster_size"] == 4]
+    assert len(clustered) == 1 and clustered[0]["expk_mode"] == hq.EXPK_SEPARABLE and clustered[0]["delay_depth"] == 16
+    assert len([t for t in table if t["cluster_size"] == 1]) == 6
+    assert sum(t["chosen"] for t in table) == 1
+    best = min(table, key=lambda t: t["ms_per_sweep"])
+    assert best["chosen"]
+    for d in (UP, DOWN):
+        a.sweep(d, hq.SWEEP_MEASURE)
+        b.sweep(d, hq.SWEEP_MEASURE)
+    for c in range(4):
+        assert np.array_equal(a.fields(c), b.fields(c)), c
+        assert np.abs(a.g(c) - b.g(c)).max() <= 1e-10 * max(1.0, np.abs(b.g(c)).max()), c
+    a.close()
+    b.close()
