@@ -134,169 +134,8 @@ k_gemm(const HqGemmJob* __restrict__ jobs, int njobs, int tiles_n) {
   }
 }
 
-// ---------------------------------------------------------------------------------
-//  k_gemm_w: the same batched products for chains of up to 144 sites (every resident
-//  lattice), one CTA per job computing the whole product in two passes over column halves
-//  of 72. Nine warps own 48 x 24 output blocks per pass (3 x 3 DMMA tiles, 36 accumulators),
-//  so a K chunk of 16 carries 36 DMMAs per warp between two barriers instead of the 12 of the
-//  48 x 48-tile kernel above, and the grid is one CTA per product. K streams through shared
-//  memory in chunks of 16 with cp.async double buffering (op(A) once per pass); the row and
-//  column scalings are formed once per CTA. Shared layouts (strides = 4 mod 16 doubles) keep
-//  the fragment loads free of bank conflicts:
-//    op(A) = A   : sA[k * kWLdm + m]     op(A) = A^T : sA[m * kWLdk + k]
-//    op(B) = B   : sB[n * kWLdk + k]     op(B) = B^T : sB[k * kWLdn + n]
-// ---------------------------------------------------------------------------------
-constexpr int kWT = 144, kWH = 72, kWKc = 16, kWLdm = 148, kWLdn = 84, kWLdk = 20, kWWarps = 9;
-constexpr int kWStageA = (kWLdm * kWKc > kWT * kWLdk) ? kWLdm * kWKc : kWT * kWLdk;  // doubles
-constexpr int kWStageB = (kWLdn * kWKc > kWH * kWLdk) ? kWLdn * kWKc : kWH * kWLdk;  // doubles
-constexpr size_t kWSmemDoubles = 2 * (size_t)kWStageA + 2 * (size_t)kWStageB + 2 * kWKc + 2 * kWT;
-
-// stages the chunk [k0, k0 + 16) x [r0, r0 + RW) of op(X) (rows r < R valid) into sX, with
-// ldr the stride of the [k][r] layout
-template <int RW>
-__device__ __forceinline__ void w_stage(const double* X, int ldx, bool kmaj, int R, int K, int r0, int k0, double* sX,
-                                        int ldr, bool pair) {
-  if (pair) {
-    if (kmaj) {
-      for (int idx = threadIdx.x; idx < RW * (kWKc / 2); idx += blockDim.x) {
-        const int r = idx / (kWKc / 2), k = 2 * (idx % (kWKc / 2));
-        const int nv = (r0 + r < R) ? min(2, K - (k0 + k)) : 0;
-        cp_async_16(sX + r * kWLdk + k, nv > 0 ? X + (k0 + k) + (size_t)(r0 + r) * ldx : X, nv);
-      }
-    } else {
-      for (int idx = threadIdx.x; idx < (RW / 2) * kWKc; idx += blockDim.x) {
-        const int r = 2 * (idx % (RW / 2)), k = idx / (RW / 2);
-        const int nv = (k0 + k < K) ? min(2, R - (r0 + r)) : 0;
-        cp_async_16(sX + k * ldr + r, nv > 0 ? X + (r0 + r) + (size_t)(k0 + k) * ldx : X, nv);
-      }
-    }
-  } else {
-    for (int idx = threadIdx.x; idx < RW * kWKc; idx += blockDim.x) {
-      int r, k;
-      if (kmaj) { r = idx / kWKc; k = idx % kWKc; } else { r = idx % RW; k = idx / RW; }
-      const bool ok = k0 + k < K && r0 + r < R;
-      const double* src = ok ? (kmaj ? X + (k0 + k) + (size_t)(r0 + r) * ldx : X + (r0 + r) + (size_t)(k0 + k) * ldx) : X;
-      cp_async_8(kmaj ? sX + r * kWLdk + k : sX + k * ldr + r, src, ok);
-    }
-  }
-}
-
-__global__ void __launch_bounds__(kWWarps * 32, 1)
-k_gemm_w(const HqGemmJob* __restrict__ jobs, int njobs) {
-  extern __shared__ __align__(16) double wsm[];
-  __shared__ double red[32];
-  const int jb = blockIdx.x;
-  if (jb >= njobs) return;
-  const HqGemmJob J = jobs[jb];
-  if (!J.active) return;
-  double* sA = wsm;                                  // [2][kWStageA]
-  double* sB = wsm + 2 * (size_t)kWStageA;           // [2][kWStageB]
-  double* sK = sB + 2 * (size_t)kWStageB;            // [2][kWKc]
-  double* rsv = sK + 2 * kWKc;                       // [kWT] row scalings
-  double* csv = rsv + kWT;                           // [kWT] column scalings
-  const bool amaj = J.ta != 0;  // op(A) = A^T is contiguous along k
-  const bool bmaj = J.tb == 0;  // op(B) = B is contiguous along k
-  const bool pa = (J.lda % 2 == 0) && ((reinterpret_cast<uintptr_t>(J.A) & 15) == 0);
-  const bool pb = (J.ldb % 2 == 0) && ((reinterpret_cast<uintptr_t>(J.B) & 15) == 0);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, q = lane & 3;
-  for (int r = threadIdx.x; r < kWT; r += blockDim.x) {
-    rsv[r] = (r < J.M) ? vscale(J.rs, J.rs_mode, r) : 0.0;
-    csv[r] = (r < J.Nc) ? vscale(J.cs, J.cs_mode, r) : 0.0;
-  }
-  const int nchunks = (J.K + kWKc - 1) / kWKc;
-  const int wm = (warp % 3) * 48;
-  const int mi = max(0, min(3, (J.M - wm + 15) / 16));  // this warp's 16-row tiles (warp-uniform)
-  double emax = -INFINITY;
-  for (int n0 = 0; n0 < J.Nc; n0 += kWH) {
-    const int wn = (warp / 3) * 24;  // within the half
-    const int nj = max(0, min(3, (J.Nc - n0 - wn + 7) / 8));
-    double acc[3][3][4];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int j = 0; j < 3; ++j) acc[i][j][0] = acc[i][j][1] = acc[i][j][2] = acc[i][j][3] = 0.0;
-    __syncthreads();  // the previous pass's last chunk is no longer read
-    w_stage<kWT>(J.A, J.lda, amaj, J.M, J.K, 0, 0, sA, kWLdm, pa);
-    w_stage<kWH>(J.B, J.ldb, bmaj, J.Nc, J.K, n0, 0, sB, kWLdn, pb);
-    if (threadIdx.x < kWKc) sK[threadIdx.x] = (threadIdx.x < J.K) ? vscale(J.ks, J.ks_mode, threadIdx.x) : 0.0;
-    cp_async_commit();
-    for (int c = 0; c < nchunks; ++c) {
-      const int cur = c & 1;
-      if (c + 1 < nchunks) {
-        const int k1 = (c + 1) * kWKc;
-        w_stage<kWT>(J.A, J.lda, amaj, J.M, J.K, 0, k1, sA + (size_t)(cur ^ 1) * kWStageA, kWLdm, pa);
-        w_stage<kWH>(J.B, J.ldb, bmaj, J.Nc, J.K, n0, k1, sB + (size_t)(cur ^ 1) * kWStageB, kWLdn, pb);
-        if (threadIdx.x < kWKc)
-          sK[(cur ^ 1) * kWKc + threadIdx.x] = (k1 + threadIdx.x < J.K) ? vscale(J.ks, J.ks_mode, k1 + threadIdx.x) : 0.0;
-      }
-      cp_async_commit();
-      cp_async_wait<1>();
-      __syncthreads();
-      const double* A_ = sA + (size_t)cur * kWStageA;
-      const double* B_ = sB + (size_t)cur * kWStageB;
-#pragma unroll
-      for (int kk = 0; kk < kWKc; kk += 4) {
-        const int k = kk + q;
-        const double ksc = sK[cur * kWKc + k];
-        double fa[3][2], fb[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          const int m = wm + 16 * i + g;
-          fa[i][0] = (amaj ? A_[m * kWLdk + k] : A_[k * kWLdm + m]) * ksc;
-          fa[i][1] = (amaj ? A_[(m + 8) * kWLdk + k] : A_[k * kWLdm + m + 8]) * ksc;
-        }
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const int n = wn + 8 * j + g;
-          fb[j] = bmaj ? B_[n * kWLdk + k] : B_[k * kWLdn + n];
-        }
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int j = 0; j < 3; ++j)
-            if (i < mi && j < nj) dmma_16x8x4(acc[i][j], fa[i][0], fa[i][1], fb[j]);
-      }
-      __syncthreads();
-    }
-    cp_async_wait<0>();
-    // epilogue of the half: alpha, row / column scalings, beta, wrap-error maximum
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int j = 0; j < 3; ++j)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int gm = wm + 16 * i + g + ((e & 2) ? 8 : 0);
-          const int gn = n0 + wn + 8 * j + 2 * q + (e & 1);
-          if (i < mi && j < nj && gm < J.M && gn < J.Nc) {
-            double v = J.alpha * acc[i][j][e] * rsv[gm] * csv[gn];
-            double* cp = J.C + gm + (size_t)gn * J.ldc;
-            const double old = (J.beta != 0.0 || J.epi == 1) ? *cp : 0.0;
-            if (J.beta != 0.0) v = fma(J.beta, old, v);
-            if (J.epi == 1) emax = fmax(emax, v - old);
-            *cp = v;
-          }
-        }
-  }
-  if (J.epi == 1 && J.err_out) {
-    emax = block_max(emax, red);
-    if (threadIdx.x == 0) atomic_max_double(J.err_out, emax);
-  }
-}
-
-cudaError_t prepare_gemm() {
-  return cudaFuncSetAttribute((const void*)k_gemm_w, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(kWSmemDoubles * sizeof(double)));
-}
-
-// products of up to 144 x 144 run one CTA per job (k_gemm_w); larger ones on 48 x 48 tiles
 cudaError_t launch_gemm(const HqGemmJob* jobs, int njobs, int Mmax, int Nmax, cudaStream_t st) {
   if (njobs <= 0) return cudaSuccess;
-  if (Mmax <= kWT && Nmax <= kWT) {
-    k_gemm_w<<<njobs, kWWarps * 32, kWSmemDoubles * sizeof(double), st>>>(jobs, njobs);
-    return cudaGetLastError();
-  }
   const int tm = (Mmax + kGT - 1) / kGT, tn = (Nmax + kGT - 1) / kGT;
   dim3 grid(tm * tn, njobs);
   k_gemm<<<grid, kGWarps * 32, 0, st>>>(jobs, njobs, tn);

@@ -424,7 +424,6 @@ cudaError_t prepare_kernels(int Nmax, int kmax, bool resident) {
   if ((e = raise_smem(3, fn_invert(), smem_invert_bytes(Nmax, resident))) != cudaSuccess) return e;
   if ((e = raise_smem(4, (const void*)k_dyn_slices, mat_stage)) != cudaSuccess) return e;
   if ((e = raise_smem(5, (const void*)k_adj_interval, mat_stage)) != cudaSuccess) return e;
-  if ((e = prepare_gemm()) != cudaSuccess) return e;
   return cudaSuccess;
 }
 

@@ -18,7 +18,6 @@ cudaError_t launch_bchain(const HqChain* chains, int n, int dir, int b, int Nmax
 cudaError_t launch_udt(const HqChain* chains, int n, int side, int b, int Nmax, bool resident, cudaStream_t st);
 cudaError_t launch_invert(const HqChain* chains, int n, int b, int which, int Nmax, bool resident, cudaStream_t st);
 cudaError_t launch_gemm(const HqGemmJob* jobs, int njobs, int Mmax, int Nmax, cudaStream_t st);
-cudaError_t prepare_gemm();
 cudaError_t launch_measure(const HqChain* chains, int n, int dir, int b, int flags, cudaStream_t st);
 cudaError_t launch_dyn_start(const HqChain* chains, int n, cudaStream_t st);
 cudaError_t launch_dyn_slices(const HqChain* chains, int n, int b, int flags, int Nmax, bool resident, cudaStream_t st);
