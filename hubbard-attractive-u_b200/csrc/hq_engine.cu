@@ -187,6 +187,7 @@ struct hq_ctx {
   // the GPU; four for larger chains, whose per-chain phases leave most SMs idle on their own)
   static constexpr int kGroups = 4;
   int ngroups = 1;
+  int gbeg[kGroups + 1] = {0, 0, 0, 0, 0};  // first chain of each group (contiguous ranges)
   cudaStream_t gstream[kGroups] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t ev_fork = nullptr, ev_join[kGroups] = {nullptr, nullptr, nullptr, nullptr};
   // the chains and stream the launch helpers currently issue for (default: all, main stream)
@@ -478,8 +479,8 @@ void in_groups(hq_ctx* c, F&& body) {
   }
   for (int g = 0; g < G; ++g) {
     if (G > 1) {
-      c->cur_c0 = (c->n * g) / G;
-      c->cur_n = (c->n * (g + 1)) / G - c->cur_c0;
+      c->cur_c0 = c->gbeg[g];
+      c->cur_n = c->gbeg[g + 1] - c->gbeg[g];
       c->cur_st = c->gstream[g];
     }
     body();
@@ -620,6 +621,22 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   if (n_chains >= 32) {
     c->ngroups = c->resident ? 2 : hq_ctx::kGroups;
     if (n_chains < 16 * c->ngroups) c->ngroups = 2;
+    // group boundaries at equal estimated work (nt N^3 per chain: the slices' wraps and
+    // flushes and the stabilisations' factorisations and products all scale so), so that
+    // uneven chains do not leave one group running alone
+    std::vector<double> pre(n_chains + 1, 0.0);
+    for (int i = 0; i < n_chains; ++i) {
+      const double N = c->ch[i].N;
+      pre[i + 1] = pre[i] + double(c->ch[i].p.nt) * N * N * N;
+    }
+    c->gbeg[0] = 0;
+    for (int g = 1; g < c->ngroups; ++g) {
+      const double target = pre[n_chains] * g / c->ngroups;
+      int k = c->gbeg[g - 1] + 1;
+      while (k < n_chains - (c->ngroups - g) && pre[k] < target) ++k;
+      c->gbeg[g] = k;
+    }
+    c->gbeg[c->ngroups] = n_chains;
     c->gstream[0] = c->stream;
     for (int g = 1; g < c->ngroups; ++g) HQ_CUDA(cudaStreamCreateWithFlags(&c->gstream[g], cudaStreamNonBlocking));
     HQ_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
