@@ -387,6 +387,44 @@ def run_gpu(args):
     if metric_wl and rank == 0 and not args.no_cpu:
         g_check = oracle_g_check(eng.g(0), eng.fields(0), params[0])
 
+    # ---- the dominant kernel alone: 128 of the chains on one stream (no chain groups), outside
+    # the timed region; its launches then occupy the GPU alone ----
+    isolated = None
+    if metric_wl and rank == 0 and dom_name == "interval" and not args.no_isolated:
+        os.environ["HQ_CHAIN_GROUPS"] = "1"
+        try:
+            solo = hq.Engine(params[:128], device=local)
+        finally:
+            os.environ.pop("HQ_CHAIN_GROUPS", None)
+        solo.fields_random()
+        solo.init()
+        sd = hq.SWEEP_UP
+        for _ in range(2):
+            solo.sweep(sd, hq.SWEEP_MEASURE)
+            sd = hq.SWEEP_DOWN if sd == hq.SWEEP_UP else hq.SWEEP_UP
+        solo.sync()
+        a0 = solo.estimators_all()
+        solo.profile_enable(True)
+        ms2 = np.zeros(len(hq.capi.PROFILE_CLASSES))
+        cnt2 = np.zeros(len(hq.capi.PROFILE_CLASSES), dtype=np.int64)
+        for _ in range(2):
+            solo.sweep(sd, hq.SWEEP_MEASURE)
+            solo.profile_collect(ms2, cnt2)
+            sd = hq.SWEEP_DOWN if sd == hq.SWEEP_UP else hq.SWEEP_UP
+        a1 = solo.estimators_all()
+        ic = hq.capi.PROFILE_CLASSES.index("interval")
+        ccfg = [solo.config(c) for c in range(128)]
+        fl = sum(interval_flops(p["nl"], p["nt"] * 2, a1[c, 5] - a0[c, 5], ccfg[c][1], ccfg[c][0])
+                 for c, p in enumerate(params[:128]))
+        launch_ms = ms2[ic] / max(1, cnt2[ic])
+        ach = fl / max(1, cnt2[ic]) / (launch_ms * 1e-3) / 1e12
+        isolated = {"chains_per_launch": 128, "launch_ms_avg": launch_ms, "achieved": ach,
+                    "frac": (ach / peak) if peak else None,
+                    "note": "k_interval timed on one stream with no other kernel beside it (a context of 128 of "
+                            "the chains with HQ_CHAIN_GROUPS=1), outside the timed region"}
+        solo.close()
+    roofline["isolated"] = isolated
+
     # ---- end to end through the C ABI from pinned host buffers: one round trip per step ----
     e2e = None
     if metric_wl and not args.no_e2e:
@@ -503,6 +541,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-single", action="store_true", help="skip the single-chain leg")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (largest delay depth, separable expK)")
+    ap.add_argument("--no-isolated", action="store_true", help="skip the dominant kernel timed alone")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

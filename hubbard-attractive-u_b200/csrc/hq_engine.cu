@@ -618,7 +618,11 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   if (hq::smem_interval_bytes(c->Nmax, c->kmax_max, c->resident) > budget)
     throw HqError(HQ_E_INVALID, "delay depth does not fit in shared memory");
   // chain groups on forked streams (see in_groups)
-  if (n_chains >= 32) {
+  // HQ_CHAIN_GROUPS=1 keeps every launch on the context stream (kernel durations without the
+  // other group's kernels beside them, for measurements)
+  const char* genv = std::getenv("HQ_CHAIN_GROUPS");
+  const bool single_group = genv && std::strcmp(genv, "1") == 0;
+  if (n_chains >= 32 && !single_group) {
     c->ngroups = c->resident ? 2 : hq_ctx::kGroups;
     if (n_chains < 16 * c->ngroups) c->ngroups = 2;
     // group boundaries at equal estimated work (nt N^3 per chain: the slices' wraps and
