@@ -601,13 +601,11 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   // ---- delay depth and shared-memory residency ----
   int smem_optin = 0;
   HQ_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
-  const size_t budget = size_t(smem_optin) - hq::max_static_smem();
-  c->resident = hq::smem_interval_bytes(c->Nmax, 4, true) <= budget &&
-                hq::smem_matrix_bytes(c->Nmax, true, 8 * (((c->Nmax + 15) & ~15) + 4) + 64) <= budget &&
-                hq::smem_invert_bytes(c->Nmax, true) <= budget && hq::smem_udt_bytes(c->Nmax, true) <= budget;
+  const size_t optin = size_t(smem_optin);
+  c->resident = hq::matrices_fit(c->Nmax, optin);
   int kfit = 4;
   for (int k : {16, 8, 4})
-    if (hq::smem_interval_bytes(c->Nmax, k, c->resident) <= budget) { kfit = k; break; }
+    if (hq::interval_fits(c->Nmax, k, c->resident, optin)) { kfit = k; break; }
   for (int i = 0; i < n_chains; ++i) {
     ChainHost& h = c->ch[i];
     // the delay depth is the site-block size of the submatrix updates: 4, 8 or 16
@@ -615,7 +613,7 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
     h.kmax = want >= 16 ? 16 : (want >= 8 ? 8 : 4);
     c->kmax_max = std::max(c->kmax_max, h.kmax);
   }
-  if (hq::smem_interval_bytes(c->Nmax, c->kmax_max, c->resident) > budget)
+  if (!hq::interval_fits(c->Nmax, c->kmax_max, c->resident, optin))
     throw HqError(HQ_E_INVALID, "delay depth does not fit in shared memory");
   // chain groups on forked streams (see in_groups)
   // HQ_CHAIN_GROUPS=1 keeps every launch on the context stream (kernel durations without the

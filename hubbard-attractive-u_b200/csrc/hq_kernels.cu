@@ -373,7 +373,8 @@ size_t smem_interval_bytes(int Nmax, int kmax, bool resident) {
   return interval_smem_doubles(Nmax, kmax, resident) * sizeof(double);
 }
 size_t smem_udt_bytes(int Nmax, bool resident) {
-  return smem_matrix_bytes(Nmax, resident, 2 * kQB * panel_ld(Nmax) + 2 * kQB * kQB + 3 * Nmax + 64);
+  return smem_matrix_bytes(Nmax, resident, 2 * kQB * panel_ld(Nmax) + 2 * kQB * kQB + 3 * Nmax + 64 +
+                                               ((Nmax - 1) / kQB) * kQB * kQB);
 }
 size_t smem_invert_bytes(int Nmax, bool resident) {
   return smem_matrix_bytes(Nmax, resident, 2 * kGJ * panel_ld(Nmax) + 3 * Nmax + 64);
@@ -403,16 +404,25 @@ static cudaError_t raise_smem(int slot, const void* fn, size_t bytes) {
 
 // sets the dynamic shared-memory limits of every per-chain kernel (outside any stream
 // capture) so that chains of up to Nmax sites can be launched
-size_t max_static_smem() {
-  const void* fns[] = {fn_interval(), (const void*)k_bchain, fn_udt(),
-                       fn_invert(), (const void*)k_dyn_slices, (const void*)k_adj_interval};
-  size_t m = 0;
-  for (const void* f : fns) {
-    cudaFuncAttributes a;
-    if (cudaFuncGetAttributes(&a, f) != cudaSuccess) return 16384;  // conservative
-    m = a.sharedSizeBytes > m ? a.sharedSizeBytes : m;
-  }
-  return m;
+// dynamic shared memory that kernel fn can take next to its own static shared memory under the
+// device's per-block opt-in limit optin
+static size_t smem_room(const void* fn, size_t optin) {
+  cudaFuncAttributes a;
+  const size_t st = cudaFuncGetAttributes(&a, fn) == cudaSuccess ? a.sharedSizeBytes : 16384;  // conservative
+  return optin > st ? optin - st : 0;
+}
+
+bool interval_fits(int Nmax, int kmax, bool resident, size_t optin) {
+  return smem_interval_bytes(Nmax, kmax, resident) <= smem_room(fn_interval(), optin);
+}
+
+bool matrices_fit(int Nmax, size_t optin) {
+  const size_t mat_stage = smem_matrix_bytes(Nmax, true, 8 * (((Nmax + 15) & ~15) + 4) + 64);
+  return interval_fits(Nmax, 4, true, optin) && mat_stage <= smem_room((const void*)k_bchain, optin) &&
+         mat_stage <= smem_room((const void*)k_dyn_slices, optin) &&
+         mat_stage <= smem_room((const void*)k_adj_interval, optin) &&
+         smem_invert_bytes(Nmax, true) <= smem_room(fn_invert(), optin) &&
+         smem_udt_bytes(Nmax, true) <= smem_room(fn_udt(), optin);
 }
 
 cudaError_t prepare_kernels(int Nmax, int kmax, bool resident) {

@@ -9,8 +9,11 @@ size_t smem_interval_bytes(int Nmax, int kmax, bool resident);
 size_t smem_matrix_bytes(int Nmax, bool resident, int extra_doubles);
 size_t smem_invert_bytes(int Nmax, bool resident);
 size_t smem_udt_bytes(int Nmax, bool resident);
-// largest static shared memory of the kernels that take dynamic shared memory
-size_t max_static_smem();
+// whether the interval kernel's dynamic shared memory for Nmax sites and delay depth kmax fits
+// next to its static shared memory under the per-block opt-in limit optin (bytes)
+bool interval_fits(int Nmax, int kmax, bool resident, size_t optin);
+// whether every per-chain kernel can keep its matrix of Nmax sites in shared memory
+bool matrices_fit(int Nmax, size_t optin);
 cudaError_t prepare_kernels(int Nmax, int kmax, bool resident);
 cudaError_t launch_interval(const HqChain* chains, int n, int dir, int b, int flags, int Nmax, int kmax, bool resident,
                             cudaStream_t st);

@@ -17,7 +17,8 @@ namespace hq {
 //  sides are long, pre-pivoting alone left the stabilised G up to ~5e-10 x max|G| from a
 //  G stabilised at every slice (12 x 12, beta = 10), the re-selection keeps it below ~4e-11,
 //  as column-pivoted QR does. Q is formed in place by the same blocks backwards
-//  (Q = B_0 B_1 ..., B_p = I - V_p T_p V_p^T).
+//  (Q = B_0 B_1 ..., B_p = I - V_p T_p V_p^T), with the T factors kept from the
+//  factorisation.
 //  Output: U (= Q) and D into stack entry b of the pushing stack, T into W0.
 // ---------------------------------------------------------------------------------
 
@@ -132,16 +133,21 @@ __device__ void qr_panel_reg(double* A, int ld, int N, int p0, int p1, double* t
   }
 }
 
-// V of the panel [p0, p0+m) with explicit unit diagonal and zeros above (columns >= m
-// zero), and the triangular factor T of H_p0 ... H_p0+m-1 = I - V T V^T
-__device__ void wy_factor(const double* A, int ld, int N, int p0, int m, const double* tau, double* Vb, int ldv,
-                          double* T, double* S) {
+// V of the panel [p0, p0+m) with explicit unit diagonal and zeros above (columns >= m zero)
+__device__ void wy_vfill(const double* A, int ld, int N, int p0, int m, double* Vb, int ldv) {
   for (int q = threadIdx.x >> 5; q < kQB; q += blockDim.x >> 5)
     for (int r = p0 + (threadIdx.x & 31); r < N; r += 32) {
       const int c = p0 + q;
       Vb[r + q * ldv] = (q >= m || r < c) ? 0.0 : (r == c ? 1.0 : A[r + (size_t)c * ld]);
     }
   __syncthreads();
+}
+
+// V of the panel [p0, p0+m) (wy_vfill) and the triangular factor T of
+// H_p0 ... H_p0+m-1 = I - V T V^T
+__device__ void wy_factor(const double* A, int ld, int N, int p0, int m, const double* tau, double* Vb, int ldv,
+                          double* T, double* S) {
+  wy_vfill(A, ld, N, p0, m, Vb, ldv);
   // S = V^T V on DMMA: warps 0 / 1 take output columns 0-7 / 8-15, four accumulator chains
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, q = lane & 3;
@@ -250,14 +256,53 @@ __device__ void wy_apply(double* A, int ld, int N, int p0, const double* Vb, int
   __syncthreads();
 }
 
-// Panel-wise column pivoting before the panel [p0, p1): the norms of the trailing columns over
-// rows p0..N-1 (the matrix as updated by the earlier panels); warp 0 then makes the p1 - p0
-// selections one after the other, each moving the remaining column of largest norm (smallest
-// index among equal norms) into the next panel position (norms and original indices swap with
-// it), and records the swaps; finally every thread applies the recorded swaps, in order, to
-// the rows it owns. piv holds kQB ints.
-__device__ void panel_pivot(double* A, int ld, int N, int p0, int p1, double* nrm, int* order, int* piv) {
+// rk[j] = the rank of column j among the columns [lo, N) in decreasing nrm, ties by position.
+// Four threads per column, each counting over one residue of positions mod 4. The norms are
+// compared as the integer patterns of their bits, which order non-negative doubles as numbers
+// and make the ranks a permutation of 0 .. N-lo-1 whatever the values (NaN included).
+__device__ void column_ranks(const double* nrm, int lo, int N, int* rk) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int nc = N - lo;
+  for (int base = warp * 32; base < 4 * nc; base += nwarps * 32) {
+    const int t = base + lane;
+    int cnt = 0;
+    if (t < 4 * nc) {
+      const int j = lo + (t >> 2);
+      const long long kj = __double_as_longlong(nrm[j]);
+      for (int i = lo + (t & 3); i < N; i += 4) {
+        const long long ki = __double_as_longlong(nrm[i]);
+        cnt += (ki > kj || (ki == kj && i < j)) ? 1 : 0;
+      }
+    }
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, 1);
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, 2);
+    if (t < 4 * nc && (t & 3) == 0) rk[lo + (t >> 2)] = cnt;
+  }
+}
+
+// Column moves of one panel pivoting step (shared memory of k_udt).
+struct PivotMoves {
+  int src[2 * kQB], dst[2 * kQB], ord[2 * kQB];
+  double nrm[2 * kQB];
+  int vac[kQB];
+  int count;
+};
+
+// Panel-wise column pivoting before the panel [p0, p1), m = p1 - p0 columns:
+//  1. the squared norms of the trailing columns over rows p0..N-1 (the matrix as updated by
+//     the earlier panels);
+//  2. the rank of every trailing column in decreasing norm, ties by position, all ranks at
+//     once (column_ranks);
+//  3. the columns of rank < m go to positions p0 + rank; the panel's other columns take the
+//     positions so vacated, both in position order (warp 0, by ballots). At most 2m columns
+//     move: they are gathered (all rows) into tmp (2 kQB columns of leading dimension ldt)
+//     and scattered to their new positions, with their norms and original indices.
+// The selected set and its order are those of m successive selections of the largest
+// remaining norm (up to the order among equal norms).
+__device__ void panel_pivot(double* A, int ld, int N, int p0, int p1, double* nrm, int* order, int* rk,
+                            double* tmp, int ldt, PivotMoves& mv) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int m = p1 - p0;
   for (int j = p0 + warp; j < N; j += nwarps) {
     double s2 = 0.0;
     for (int r = p0 + lane; r < N; r += 32) {
@@ -268,41 +313,64 @@ __device__ void panel_pivot(double* A, int ld, int N, int p0, int p1, double* nr
     if (lane == 0) nrm[j] = s2;
   }
   __syncthreads();
+  column_ranks(nrm, p0, N, rk);
+  __syncthreads();
   if (warp == 0) {
-    for (int q = p0; q < p1; ++q) {
-      double best = -1.0;
-      int bj = N;
-      for (int j = q + lane; j < N; j += 32) {
-        const double v = nrm[j];
-        if (v > best) { best = v; bj = j; }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oj = __shfl_xor_sync(0xffffffffu, bj, o);
-        if (ob > best || (ob == best && oj < bj)) { best = ob; bj = oj; }
-      }
-      if (bj >= N) bj = q;
-      if (lane == 0) {
-        piv[q - p0] = bj;
-        if (bj != q) {
-          const double tn = nrm[q]; nrm[q] = nrm[bj]; nrm[bj] = tn;
-          const int to = order[q]; order[q] = order[bj]; order[bj] = to;
-        }
-      }
-      __syncwarp();
+    const unsigned below = (1u << lane) - 1u;
+    int nvac = 0;
+    for (int base = p1; base < N; base += 32) {
+      const int j = base + lane;
+      const bool v = j < N && rk[j] < m;
+      const unsigned b = __ballot_sync(0xffffffffu, v);
+      const int s = nvac + __popc(b & below);
+      if (v && s < kQB) mv.vac[s] = j;
+      nvac += __popc(b);
     }
+    __syncwarp();
+    int ndisp = 0, nmv = 0;
+    for (int base = p0; base < N; base += 32) {
+      const int j = base + lane;
+      int np = j;
+      bool disp = false;
+      if (j < N) {
+        const int r = rk[j];
+        if (r < m) np = p0 + r;
+        else if (j < p1) disp = true;
+      }
+      const unsigned bd = __ballot_sync(0xffffffffu, disp);
+      if (disp) {
+        const int s = ndisp + __popc(bd & below);
+        np = (s < nvac && s < kQB) ? mv.vac[s] : j;
+      }
+      ndisp += __popc(bd);
+      const bool moves = j < N && np != j;
+      const unsigned bm = __ballot_sync(0xffffffffu, moves);
+      const int s = nmv + __popc(bm & below);
+      if (moves && s < 2 * kQB) {
+        mv.src[s] = j;
+        mv.dst[s] = np;
+        mv.nrm[s] = nrm[j];
+        mv.ord[s] = order[j];
+      }
+      nmv += __popc(bm);
+    }
+    if (lane == 0) mv.count = min(nmv, 2 * kQB);
   }
   __syncthreads();
-  for (int r = threadIdx.x; r < N; r += blockDim.x)
-    for (int q = p0; q < p1; ++q) {
-      const int jp = piv[q - p0];
-      if (jp != q) {
-        const double t0 = A[r + (size_t)q * ld];
-        A[r + (size_t)q * ld] = A[r + (size_t)jp * ld];
-        A[r + (size_t)jp * ld] = t0;
-      }
+  const int nmv = mv.count;
+  for (int t = warp; t < nmv; t += nwarps) {
+    const double* s = A + (size_t)mv.src[t] * ld;
+    for (int r = lane; r < N; r += 32) tmp[r + (size_t)t * ldt] = s[r];
+  }
+  __syncthreads();
+  for (int t = warp; t < nmv; t += nwarps) {
+    double* d = A + (size_t)mv.dst[t] * ld;
+    for (int r = lane; r < N; r += 32) d[r] = tmp[r + (size_t)t * ldt];
+    if (lane == 0) {
+      nrm[mv.dst[t]] = mv.nrm[t];
+      order[mv.dst[t]] = mv.ord[t];
     }
+  }
   __syncthreads();
 }
 
@@ -330,6 +398,12 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
   double* tau = p; p += N;
   double* nrm = p; p += N;
   int* order = reinterpret_cast<int*>(p);
+  int* rk = order + N;
+  p += N;
+  // T factors of the panels that have trailing columns, kept from the factorisation for the
+  // formation of Q (panel i at Tc + i kQB^2)
+  double* Tc = p;
+  __shared__ PivotMoves mv;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const double* X = ch.X;
   // ---- pre-pivoting: columns by decreasing norm (ties by index) ----
@@ -340,15 +414,9 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
     if (lane == 0) nrm[j] = s2;
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < N; j += blockDim.x) {
-    const double nj = nrm[j];
-    int rank = 0;
-    for (int i = 0; i < N; ++i) {
-      const double ni = nrm[i];
-      rank += (ni > nj || (ni == nj && i < j)) ? 1 : 0;
-    }
-    order[rank] = j;
-  }
+  column_ranks(nrm, 0, N, rk);
+  __syncthreads();
+  for (int j = threadIdx.x; j < N; j += blockDim.x) order[rk[j]] = j;
   __syncthreads();
   if (resident) {
     HQ_FOR_EACH_ELEM(N, i, j) cp_async_8(A + i + (size_t)j * ld, X + i + (size_t)order[j] * N, true);
@@ -359,15 +427,15 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
   }
   __syncthreads();
   // ---- blocked Householder QR ----
-  __shared__ int piv[kQB];
   for (int p0 = 0; p0 < N; p0 += kQB) {
     const int p1 = min(p0 + kQB, N);
-    if (p0 > 0) panel_pivot(A, ld, N, p0, p1, nrm, order, piv);
+    if (p0 > 0) panel_pivot(A, ld, N, p0, p1, nrm, order, rk, Vb, ldp, mv);
     if (N <= 160) qr_panel_reg<5>(A, ld, N, p0, p1, tau);
     else qr_panel(A, ld, N, p0, p1, tau);
     if (p1 < N) {
-      wy_factor(A, ld, N, p0, p1 - p0, tau, Vb, ldp, T, S);
-      wy_apply(A, ld, N, p0, Vb, ldp, T, true, W, ldp, p1, N - p1);
+      double* Tp = Tc + (size_t)(p0 / kQB) * kQB * kQB;
+      wy_factor(A, ld, N, p0, p1 - p0, tau, Vb, ldp, Tp, S);
+      wy_apply(A, ld, N, p0, Vb, ldp, Tp, true, W, ldp, p1, N - p1);
     }
   }
   // ---- D = |diag R|, T = D^-1 R P^T (T[:, order[c]] = row-scaled R[:, c]) ----
@@ -390,13 +458,19 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
   //   Q[:, p0:p1] = E - V T V[p0:p1, :]^T ----
   for (int p0 = ((N - 1) / kQB) * kQB; p0 >= 0; p0 -= kQB) {
     const int p1 = min(p0 + kQB, N), m = p1 - p0;
-    wy_factor(A, ld, N, p0, m, tau, Vb, ldp, T, S);
-    if (p1 < N) wy_apply(A, ld, N, p0, Vb, ldp, T, false, W, ldp, p1, N - p1);
+    const double* Tp = T;
+    if (p1 < N) {
+      Tp = Tc + (size_t)(p0 / kQB) * kQB * kQB;
+      wy_vfill(A, ld, N, p0, m, Vb, ldp);
+      wy_apply(A, ld, N, p0, Vb, ldp, Tp, false, W, ldp, p1, N - p1);
+    } else {
+      wy_factor(A, ld, N, p0, m, tau, Vb, ldp, T, S);
+    }
     for (int t = threadIdx.x; t < kQB * kQB; t += blockDim.x) {
       const int l = t / kQB, j = t % kQB;
       double acc = 0.0;
       if (j < m)
-        for (int l2 = 0; l2 < kQB; ++l2) acc = fma(T[l * kQB + l2], Vb[(p0 + j) + l2 * ldp], acc);
+        for (int l2 = 0; l2 < kQB; ++l2) acc = fma(Tp[l * kQB + l2], Vb[(p0 + j) + l2 * ldp], acc);
       W[l * ldp + j] = -acc;
     }
     for (int idx = threadIdx.x; idx < N * m; idx += blockDim.x) {
