@@ -143,74 +143,77 @@ __device__ void wy_vfill(const double* A, int ld, int N, int p0, int m, double* 
   __syncthreads();
 }
 
+// S = V^T V (kQB x kQB) on DMMA, by warps 0 and 1 only (output columns 0-7 / 8-15), four
+// accumulator chains
+__device__ __forceinline__ void wy_gram(int N, int p0, const double* Vb, int ldv, double* S) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int n0 = warp * 8;
+  double acc[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
+  for (int r0 = p0; r0 < N; r0 += 16) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int r = r0 + 4 * u + q;
+      const bool ok = r < N;
+      const double a0 = ok ? Vb[r + g * ldv] : 0.0;
+      const double a1 = ok ? Vb[r + (g + 8) * ldv] : 0.0;
+      const double b0 = ok ? Vb[r + (n0 + g) * ldv] : 0.0;
+      dmma_16x8x4(acc[u], a0, a1, b0);
+    }
+  }
+  const int cc = n0 + 2 * q;
+  S[g * kQB + cc] = (acc[0][0] + acc[1][0]) + (acc[2][0] + acc[3][0]);
+  S[g * kQB + cc + 1] = (acc[0][1] + acc[1][1]) + (acc[2][1] + acc[3][1]);
+  S[(g + 8) * kQB + cc] = (acc[0][2] + acc[1][2]) + (acc[2][2] + acc[3][2]);
+  S[(g + 8) * kQB + cc + 1] = (acc[0][3] + acc[1][3]) + (acc[2][3] + acc[3][3]);
+}
+
+// T[i][j] = -tau_j sum_{i <= l < j} T[i][l] S[l][j], T[i][i] = tau_i (columns j >= m zero), by
+// warp 0 only: lane i keeps row i. Every lane runs the same instructions (t[l] = 0 for l < i,
+// entries off the upper triangle selected to zero), so the loads of S and tau issue ahead of
+// the recurrence.
+__device__ __forceinline__ void wy_tfactor(int p0, int m, const double* tau, const double* S, double* T) {
+  const int i = threadIdx.x & 31;
+  double t[kQB];
+#pragma unroll
+  for (int j = 0; j < kQB; ++j) {
+    const double tj = (j < m) ? tau[p0 + j] : 0.0;
+    double acc0 = 0.0, acc1 = 0.0;  // two chains
+#pragma unroll
+    for (int l = 0; l < j; l += 2) {
+      acc0 = fma(t[l], S[l * kQB + j], acc0);
+      if (l + 1 < j) acc1 = fma(t[l + 1], S[(l + 1) * kQB + j], acc1);
+    }
+    const double v = -tj * (acc0 + acc1);
+    t[j] = (j >= m) ? 0.0 : (i == j ? tj : (i < j ? v : 0.0));
+  }
+  if (i < kQB) {
+#pragma unroll
+    for (int j = 0; j < kQB; ++j) T[i * kQB + j] = t[j];
+  }
+}
+
 // V of the panel [p0, p0+m) (wy_vfill) and the triangular factor T of
 // H_p0 ... H_p0+m-1 = I - V T V^T
 __device__ void wy_factor(const double* A, int ld, int N, int p0, int m, const double* tau, double* Vb, int ldv,
                           double* T, double* S) {
   wy_vfill(A, ld, N, p0, m, Vb, ldv);
-  // S = V^T V on DMMA: warps 0 / 1 take output columns 0-7 / 8-15, four accumulator chains
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, q = lane & 3;
-  if (warp < 2) {
-    const int n0 = warp * 8;
-    double acc[4][4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
-    for (int r0 = p0; r0 < N; r0 += 16) {
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int r = r0 + 4 * u + q;
-        const bool ok = r < N;
-        const double a0 = ok ? Vb[r + g * ldv] : 0.0;
-        const double a1 = ok ? Vb[r + (g + 8) * ldv] : 0.0;
-        const double b0 = ok ? Vb[r + (n0 + g) * ldv] : 0.0;
-        dmma_16x8x4(acc[u], a0, a1, b0);
-      }
-    }
-    const int cc = n0 + 2 * q;
-    S[g * kQB + cc] = (acc[0][0] + acc[1][0]) + (acc[2][0] + acc[3][0]);
-    S[g * kQB + cc + 1] = (acc[0][1] + acc[1][1]) + (acc[2][1] + acc[3][1]);
-    S[(g + 8) * kQB + cc] = (acc[0][2] + acc[1][2]) + (acc[2][2] + acc[3][2]);
-    S[(g + 8) * kQB + cc + 1] = (acc[0][3] + acc[1][3]) + (acc[2][3] + acc[3][3]);
-  }
+  if ((threadIdx.x >> 5) < 2) wy_gram(N, p0, Vb, ldv, S);
   __syncthreads();
-  // T[i][j] = -tau_j sum_{i <= l < j} T[i][l] S[l][j] (T[i][i] = tau_i): lane i keeps row i
-  if (warp == 0 && lane < kQB) {
-    const int i = lane;
-    double t[kQB];
-#pragma unroll
-    for (int j = 0; j < kQB; ++j) {
-      double v = 0.0;
-      if (j < m) {
-        if (i == j) {
-          v = tau[p0 + j];
-        } else if (i < j) {
-          double acc0 = 0.0, acc1 = 0.0;  // t[l] = 0 for l < i; two chains
-#pragma unroll
-          for (int l = 0; l < j; l += 2) {
-            acc0 = fma(t[l], S[l * kQB + j], acc0);
-            if (l + 1 < j) acc1 = fma(t[l + 1], S[(l + 1) * kQB + j], acc1);
-          }
-          v = -tau[p0 + j] * (acc0 + acc1);
-        }
-      }
-      t[j] = v;
-    }
-#pragma unroll
-    for (int j = 0; j < kQB; ++j) T[i * kQB + j] = t[j];
-  }
+  if ((threadIdx.x >> 5) == 0) wy_tfactor(p0, m, tau, S, T);
   __syncthreads();
 }
 
-// A[p0:, col0:col0+nc] <- (I - V op(T) V^T) A[p0:, col0:col0+nc]; op(T) = T^T if trans
-__device__ void wy_apply(double* A, int ld, int N, int p0, const double* Vb, int ldv, const double* T, bool trans,
-                         double* W, int ldw, int col0, int nc) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+// W = V^T A_sub (kQB x nc, A_sub = A[p0:, col0:col0+nc]) with DMMA: m16 = the panel columns,
+// k = rows p0..N-1, four accumulator chains per 8-column tile; tiles over warps w0, w0 + ws, ...
+__device__ __forceinline__ void wy_vta(const double* A, int ld, int N, int p0, const double* Vb, int ldv, double* W,
+                                       int ldw, int col0, int nc, int w0, int ws) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, q = lane & 3;
-  // W = V^T A_sub (kQB x nc) with DMMA: m16 = the panel columns, k = rows p0..N-1, four
-  // accumulator chains per 8-column tile
   const int nt8 = (nc + 7) / 8;
-  for (int t = warp; t < nt8; t += nwarps) {
+  for (int t = warp - w0; t < nt8; t += ws) {
     const int cb = t * 8 + g;
     double acc[4][4];
 #pragma unroll
@@ -231,8 +234,15 @@ __device__ void wy_apply(double* A, int ld, int N, int p0, const double* Vb, int
     if (c < nc) { W[g * ldw + c] = acc[0][0]; W[(g + 8) * ldw + c] = acc[0][2]; }
     if (c + 1 < nc) { W[g * ldw + c + 1] = acc[0][1]; W[(g + 8) * ldw + c + 1] = acc[0][3]; }
   }
-  __syncthreads();
-  // W <- -op(T) W by DMMA, in place per 8-column tile (a tile's loads precede its stores)
+}
+
+// W <- -op(T) W (op(T) = T^T if trans) by DMMA, in place per 8-column tile (a tile's loads
+// precede its stores), then A_sub += V W; W = V^T A_sub on entry, after a block barrier
+__device__ void wy_tw_rank(double* A, int ld, int N, int p0, const double* Vb, int ldv, const double* T, bool trans,
+                           double* W, int ldw, int col0, int nc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int nt8 = (nc + 7) / 8;
   for (int t = warp; t < nt8; t += nwarps) {
     const int n = t * 8 + g;
     double bw[4];
@@ -251,16 +261,42 @@ __device__ void wy_apply(double* A, int ld, int N, int p0, const double* Vb, int
     if (c + 1 < nc) { W[g * ldw + c + 1] = -acc[1]; W[(g + 8) * ldw + c + 1] = -acc[3]; }
   }
   __syncthreads();
-  // A_sub += V (-op(T) W)
   rank_update(A + p0 + (size_t)col0 * ld, ld, N - p0, nc, Vb + p0, ldv, W, ldw, kQB);
   __syncthreads();
 }
 
-// rk[j] = the rank of column j among the columns [lo, N) in decreasing nrm, ties by position.
-// Four threads per column, each counting over one residue of positions mod 4. The norms are
-// compared as the integer patterns of their bits, which order non-negative doubles as numbers
-// and make the ranks a permutation of 0 .. N-lo-1 whatever the values (NaN included).
-__device__ void column_ranks(const double* nrm, int lo, int N, int* rk) {
+// A[p0:, col0:col0+nc] <- (I - V op(T) V^T) A[p0:, col0:col0+nc]; op(T) = T^T if trans
+__device__ void wy_apply(double* A, int ld, int N, int p0, const double* Vb, int ldv, const double* T, bool trans,
+                         double* W, int ldw, int col0, int nc) {
+  wy_vta(A, ld, N, p0, Vb, ldv, W, ldw, col0, nc, 0, blockDim.x >> 5);
+  __syncthreads();
+  wy_tw_rank(A, ld, N, p0, Vb, ldv, T, trans, W, ldw, col0, nc);
+}
+
+// The trailing update of the factorisation, A_sub <- (I - V T^T V^T) A_sub with the panel's
+// T formed on the way: warps 0 and 1 form S = V^T V and warp 0 then T (two-warp named
+// barrier between them), while the other warps form W = V^T A_sub, which does not need T.
+__device__ void wy_forward(double* A, int ld, int N, int p0, int m, const double* tau, double* Vb, int ldv, double* T,
+                           double* S, double* W, int ldw, int col0, int nc) {
+  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  wy_vfill(A, ld, N, p0, m, Vb, ldv);
+  if (warp < 2) {
+    wy_gram(N, p0, Vb, ldv, S);
+    asm volatile("bar.sync 1, 64;" ::: "memory");
+    if (warp == 0) wy_tfactor(p0, m, tau, S, T);
+  } else {
+    wy_vta(A, ld, N, p0, Vb, ldv, W, ldw, col0, nc, 2, nwarps - 2);
+  }
+  __syncthreads();
+  wy_tw_rank(A, ld, N, p0, Vb, ldv, T, true, W, ldw, col0, nc);
+}
+
+// rk[j] = the rank of column j among the columns [lo, N) in decreasing nrm, ties by position,
+// and who[r] = the column of rank r for r < m. Four threads per column, each counting over one
+// residue of positions mod 4. The norms are compared as the integer patterns of their bits,
+// which order non-negative doubles as numbers and make the ranks a permutation of
+// 0 .. N-lo-1 whatever the values (NaN included).
+__device__ void column_ranks(const double* nrm, int lo, int N, int* rk, int m, int* who) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int nc = N - lo;
   for (int base = warp * 32; base < 4 * nc; base += nwarps * 32) {
@@ -269,106 +305,123 @@ __device__ void column_ranks(const double* nrm, int lo, int N, int* rk) {
     if (t < 4 * nc) {
       const int j = lo + (t >> 2);
       const long long kj = __double_as_longlong(nrm[j]);
-      for (int i = lo + (t & 3); i < N; i += 4) {
-        const long long ki = __double_as_longlong(nrm[i]);
-        cnt += (ki > kj || (ki == kj && i < j)) ? 1 : 0;
-      }
+      int i = lo + (t & 3);
+#pragma unroll 4
+      for (; i < j; i += 4) cnt += __double_as_longlong(nrm[i]) >= kj ? 1 : 0;  // ahead of j: ties count
+#pragma unroll 4
+      for (; i < N; i += 4) cnt += __double_as_longlong(nrm[i]) > kj ? 1 : 0;   // j itself and behind
     }
     cnt += __shfl_xor_sync(0xffffffffu, cnt, 1);
     cnt += __shfl_xor_sync(0xffffffffu, cnt, 2);
-    if (t < 4 * nc && (t & 3) == 0) rk[lo + (t >> 2)] = cnt;
+    if (t < 4 * nc && (t & 3) == 0) {
+      rk[lo + (t >> 2)] = cnt;
+      if (cnt < m) who[cnt] = lo + (t >> 2);
+    }
   }
 }
 
-// Column moves of one panel pivoting step (shared memory of k_udt).
+// Column moves of one panel pivoting step (shared memory of k_udt): who[r] = the column of
+// rank r; per tmp slot the new position of the column saved there (-1: the slot is unused),
+// its norm and its original index.
 struct PivotMoves {
-  int src[2 * kQB], dst[2 * kQB], ord[2 * kQB];
+  int who[kQB];
+  int dst[2 * kQB], ord[2 * kQB];
   double nrm[2 * kQB];
-  int vac[kQB];
-  int count;
 };
 
 // Panel-wise column pivoting before the panel [p0, p1), m = p1 - p0 columns:
 //  1. the squared norms of the trailing columns over rows p0..N-1 (the matrix as updated by
-//     the earlier panels);
-//  2. the rank of every trailing column in decreasing norm, ties by position, all ranks at
-//     once (column_ranks);
-//  3. the columns of rank < m go to positions p0 + rank; the panel's other columns take the
-//     positions so vacated, both in position order (warp 0, by ballots). At most 2m columns
-//     move: they are gathered (all rows) into tmp (2 kQB columns of leading dimension ldt)
-//     and scattered to their new positions, with their norms and original indices.
+//     the earlier panels); a warp takes four columns at a time, so that their loads and warp
+//     reductions overlap (all RPL rows per lane unrolled when RPL > 0, N <= 32 RPL);
+//  2. the rank of every trailing column in decreasing norm, ties by position (column_ranks);
+//  3. the column of rank r < m goes to position p0 + r. A panel column of rank >= m goes to a
+//     position vacated by a selected column outside the panel: the end of its chain w, the
+//     column that moves to w, the column that moves to that one's position, ..., which
+//     leaves the panel within m steps. The moving columns (at most 2m) are saved in tmp
+//     (2 kQB columns of leading dimension ldt; slot r for rank r, slot m + w - p0 for panel
+//     position w) and then written to their new positions with their norms and original
+//     indices.
 // The selected set and its order are those of m successive selections of the largest
 // remaining norm (up to the order among equal norms).
+template <int RPL>
 __device__ void panel_pivot(double* A, int ld, int N, int p0, int p1, double* nrm, int* order, int* rk,
                             double* tmp, int ldt, PivotMoves& mv) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int m = p1 - p0;
-  for (int j = p0 + warp; j < N; j += nwarps) {
-    double s2 = 0.0;
-    for (int r = p0 + lane; r < N; r += 32) {
-      const double v = A[r + (size_t)j * ld];
-      s2 = fma(v, v, s2);
-    }
-    s2 = warp_sum(s2);
-    if (lane == 0) nrm[j] = s2;
-  }
-  __syncthreads();
-  column_ranks(nrm, p0, N, rk);
-  __syncthreads();
-  if (warp == 0) {
-    const unsigned below = (1u << lane) - 1u;
-    int nvac = 0;
-    for (int base = p1; base < N; base += 32) {
-      const int j = base + lane;
-      const bool v = j < N && rk[j] < m;
-      const unsigned b = __ballot_sync(0xffffffffu, v);
-      const int s = nvac + __popc(b & below);
-      if (v && s < kQB) mv.vac[s] = j;
-      nvac += __popc(b);
-    }
-    __syncwarp();
-    int ndisp = 0, nmv = 0;
-    for (int base = p0; base < N; base += 32) {
-      const int j = base + lane;
-      int np = j;
-      bool disp = false;
-      if (j < N) {
-        const int r = rk[j];
-        if (r < m) np = p0 + r;
-        else if (j < p1) disp = true;
+  // warp w takes columns p0 + w, p0 + w + nwarps, ..., four at a time
+  for (int j0 = p0 + warp; j0 < N; j0 += 4 * nwarps) {
+    double s2[4] = {0.0, 0.0, 0.0, 0.0};
+    if (RPL > 0) {
+#pragma unroll
+      for (int t = 0; t < (RPL > 0 ? RPL : 1); ++t) {
+        const int r = p0 + lane + 32 * t;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int j = j0 + u * nwarps;
+          if (r < N && j < N) {
+            const double v = A[r + (size_t)j * ld];
+            s2[u] = fma(v, v, s2[u]);
+          }
+        }
       }
-      const unsigned bd = __ballot_sync(0xffffffffu, disp);
-      if (disp) {
-        const int s = ndisp + __popc(bd & below);
-        np = (s < nvac && s < kQB) ? mv.vac[s] : j;
+    } else {
+      for (int r = p0 + lane; r < N; r += 32) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int j = j0 + u * nwarps;
+          if (j < N) {
+            const double v = A[r + (size_t)j * ld];
+            s2[u] = fma(v, v, s2[u]);
+          }
+        }
       }
-      ndisp += __popc(bd);
-      const bool moves = j < N && np != j;
-      const unsigned bm = __ballot_sync(0xffffffffu, moves);
-      const int s = nmv + __popc(bm & below);
-      if (moves && s < 2 * kQB) {
-        mv.src[s] = j;
-        mv.dst[s] = np;
-        mv.nrm[s] = nrm[j];
-        mv.ord[s] = order[j];
-      }
-      nmv += __popc(bm);
     }
-    if (lane == 0) mv.count = min(nmv, 2 * kQB);
-  }
-  __syncthreads();
-  const int nmv = mv.count;
-  for (int t = warp; t < nmv; t += nwarps) {
-    const double* s = A + (size_t)mv.src[t] * ld;
-    for (int r = lane; r < N; r += 32) tmp[r + (size_t)t * ldt] = s[r];
-  }
-  __syncthreads();
-  for (int t = warp; t < nmv; t += nwarps) {
-    double* d = A + (size_t)mv.dst[t] * ld;
-    for (int r = lane; r < N; r += 32) d[r] = tmp[r + (size_t)t * ldt];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) s2[u] = warp_sum(s2[u]);
     if (lane == 0) {
-      nrm[mv.dst[t]] = mv.nrm[t];
-      order[mv.dst[t]] = mv.ord[t];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (j0 + u * nwarps < N) nrm[j0 + u * nwarps] = s2[u];
+    }
+  }
+  __syncthreads();
+  column_ranks(nrm, p0, N, rk, m, mv.who);
+  __syncthreads();
+  for (int j = p0 + warp; j < N; j += nwarps) {  // uniform per warp
+    const int r = rk[j];
+    int slot = -1, np = j;
+    if (r < m) {
+      slot = r;
+      np = p0 + r;
+    } else if (j < p1) {
+      slot = m + (j - p0);
+      int x = mv.who[j - p0];
+      for (int it = 0; it < kQB && x >= p0 && x < p1; ++it) x = mv.who[x - p0];
+      np = x;
+    }
+    if (slot >= 0 && np != j) {
+      const double* src = A + (size_t)j * ld;
+      for (int rr = lane; rr < N; rr += 32) tmp[rr + (size_t)slot * ldt] = src[rr];
+    }
+    if (lane == 0) {
+      if (slot >= 0) {
+        mv.dst[slot] = np != j ? np : -1;
+        mv.nrm[slot] = nrm[j];
+        mv.ord[slot] = order[j];
+      }
+      if (j < p1 && slot < m) mv.dst[m + (j - p0)] = -1;  // a selected panel column: its slot is free
+    }
+  }
+  __syncthreads();
+  for (int sl = warp; sl < 2 * m; sl += nwarps) {
+    const int d = mv.dst[sl];
+    if (d >= 0) {
+      double* dc = A + (size_t)d * ld;
+      for (int rr = lane; rr < N; rr += 32) dc[rr] = tmp[rr + (size_t)sl * ldt];
+      if (lane == 0) {
+        nrm[d] = mv.nrm[sl];
+        order[d] = mv.ord[sl];
+      }
     }
   }
   __syncthreads();
@@ -404,38 +457,31 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
   // formation of Q (panel i at Tc + i kQB^2)
   double* Tc = p;
   __shared__ PivotMoves mv;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const double* X = ch.X;
-  // ---- pre-pivoting: columns by decreasing norm (ties by index) ----
-  for (int j = warp; j < N; j += nwarps) {
-    double s2 = 0.0;
-    for (int i = lane; i < N; i += 32) { const double v = X[i + (size_t)j * N]; s2 = fma(v, v, s2); }
-    s2 = warp_sum(s2);
-    if (lane == 0) nrm[j] = s2;
-  }
-  __syncthreads();
-  column_ranks(nrm, 0, N, rk);
-  __syncthreads();
-  for (int j = threadIdx.x; j < N; j += blockDim.x) order[rk[j]] = j;
-  __syncthreads();
   if (resident) {
-    HQ_FOR_EACH_ELEM(N, i, j) cp_async_8(A + i + (size_t)j * ld, X + i + (size_t)order[j] * N, true);
+    HQ_FOR_EACH_ELEM(N, i, j) cp_async_8(A + i + (size_t)j * ld, X + i + (size_t)j * N, true);
     cp_async_commit();
-    cp_async_wait<0>();
   } else {
-    HQ_FOR_EACH_ELEM(N, i, j) A[i + (size_t)j * ld] = X[i + (size_t)order[j] * N];
+    HQ_FOR_EACH_ELEM(N, i, j) A[i + (size_t)j * ld] = X[i + (size_t)j * N];
   }
+  for (int j = threadIdx.x; j < N; j += blockDim.x) order[j] = j;
+  if (resident) cp_async_wait<0>();
   __syncthreads();
-  // ---- blocked Householder QR ----
+  // ---- blocked Householder QR; the pivoting of the first panel is the pre-pivoting (its 16
+  // columns are the first 16 of the columns sorted by decreasing norm; the order of the
+  // others does not matter, as every later panel selects by norm again) ----
   for (int p0 = 0; p0 < N; p0 += kQB) {
     const int p1 = min(p0 + kQB, N);
-    if (p0 > 0) panel_pivot(A, ld, N, p0, p1, nrm, order, rk, Vb, ldp, mv);
-    if (N <= 160) qr_panel_reg<5>(A, ld, N, p0, p1, tau);
-    else qr_panel(A, ld, N, p0, p1, tau);
+    if (N <= 160) {
+      panel_pivot<5>(A, ld, N, p0, p1, nrm, order, rk, Vb, ldp, mv);
+      qr_panel_reg<5>(A, ld, N, p0, p1, tau);
+    } else {
+      panel_pivot<0>(A, ld, N, p0, p1, nrm, order, rk, Vb, ldp, mv);
+      qr_panel(A, ld, N, p0, p1, tau);
+    }
     if (p1 < N) {
       double* Tp = Tc + (size_t)(p0 / kQB) * kQB * kQB;
-      wy_factor(A, ld, N, p0, p1 - p0, tau, Vb, ldp, Tp, S);
-      wy_apply(A, ld, N, p0, Vb, ldp, Tp, true, W, ldp, p1, N - p1);
+      wy_forward(A, ld, N, p0, p1 - p0, tau, Vb, ldp, Tp, S, W, ldp, p1, N - p1);
     }
   }
   // ---- D = |diag R|, T = D^-1 R P^T (T[:, order[c]] = row-scaled R[:, c]) ----
@@ -445,12 +491,13 @@ k_udt(const HqChain* __restrict__ chains, int nchains, int side, int unused, int
   for (int r = threadIdx.x; r < N; r += blockDim.x) {
     const double dr = fabs(A[r + (size_t)r * ld]);
     Dout[r] = dr;
-    nrm[r] = dr;
+    nrm[r] = dr != 0.0 ? 1.0 / dr : 0.0;  // row scale of T; 0 marks a zero row of R
   }
   __syncthreads();
   HQ_FOR_EACH_ELEM(N, r, cc) {
-    const double v = (r <= cc) ? A[r + (size_t)cc * ld] / nrm[r] : 0.0;
-    Tout[r + (size_t)order[cc] * N] = (nrm[r] != 0.0) ? v : (r == cc ? 1.0 : 0.0);
+    const double ir = nrm[r];
+    const double v = (r <= cc) ? A[r + (size_t)cc * ld] * ir : 0.0;
+    Tout[r + (size_t)order[cc] * N] = (ir != 0.0) ? v : (r == cc ? 1.0 : 0.0);
   }
   __syncthreads();
   // ---- form Q in place, panels backwards: the trailing columns get the panel's WY
