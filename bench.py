@@ -271,6 +271,20 @@ def interval_flops(nl, n_slices, accepted, kmax, expk_mode):
     return n_slices * wrap + accepted * flip
 
 
+def sweep_flops(p, sweeps, accepted, kmax, expk_mode):
+    """Algorithmic FP64 flops of whole directional sweeps of one chain, as the persistent sweep
+    kernel performs them: the interval work (interval_flops) plus, per stabilisation interval,
+    the B chain of its slices (4 N L^3 per slice separable, 2 N^3 dense), the UDV factorisation
+    with the formation of Q (8/3 N^3), the cumulative V^T (2 N^3), the four builder products
+    (8 N^3) and the inverse (2 N^3)."""
+    nl, nt = p["nl"], p["nt"]
+    N = nl * nl
+    n_stab = -(-nt // p["stabilization_pace"])
+    bchain = (4.0 * N * nl ** 3) if expk_mode == 1 else (2.0 * N ** 3)
+    stab = sweeps * (nt * bchain + n_stab * (8.0 / 3.0 + 2.0 + 8.0 + 2.0) * N ** 3)
+    return interval_flops(nl, nt * sweeps, accepted, kmax, expk_mode) + stab
+
+
 def dense_equivalent_flops(p, sweeps, accepted):
     """One chain's sweeps in the dense-GEMM convention: nt 6N^3 + n_stab 33N^3 per sweep and
     2N^2 per accepted flip."""
@@ -357,6 +371,9 @@ def run_gpu(args):
         flops_total = sum(interval_flops(p["nl"], p["nt"] * args.steps, acc_chain[c], cfgs[c][1], cfgs[c][0])
                           for c, p in enumerate(params))
         flops_per_launch = flops_total / max(1, cnt_cls[dom])
+    elif dom_name == "sweep":
+        flops_total = sum(sweep_flops(p, args.steps, acc_chain[c], cfgs[c][1], cfgs[c][0]) for c, p in enumerate(params))
+        flops_per_launch = flops_total / max(1, cnt_cls[dom])
     else:
         flops_per_launch = None
     achieved = (flops_per_launch / (avg_launch_ms * 1e-3) / 1e12) if flops_per_launch else None
@@ -369,10 +386,15 @@ def run_gpu(args):
         traffic = 2.864e6 * chains_per_launch / 16
     f_sweep = world * sum(dense_equivalent_flops(p, args.steps, acc_chain[c]) for c, p in enumerate(params))
     sweep_tf = f_sweep / (ms * 1e-3) / 1e12
+    sweep_mode = "persistent" if eng.sweep_mode() == hq.SWEEP_PERSISTENT else "launches"
     roofline = {"bound": "tensor", "kernel": f"k_{dom_name}", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
                 "traffic_source": ("ncu dram__bytes_read+write of one k_interval launch of 16 chains, scaled by chains"
                                    if traffic else None),
+                "flops_convention": ("whole sweep: interval work (separable wrap 8NL^3 per slice, 2N^2 + 4N m per "
+                                     "accepted flip) + per interval B chain, UDV 8/3 N^3, V^T 2N^3, builder 8N^3, "
+                                     "inverse 2N^3" if dom_name == "sweep" else
+                                     "interval work: separable wrap 8NL^3 per slice, 2N^2 + 4N m per accepted flip"),
                 "sweep_dense_equivalent": {"tflops": sweep_tf, "frac": (sweep_tf / peak) if peak else None,
                                            "convention": "F = nt*6N^3 + 2N^2*accepted + n_stab*33N^3 per chain-sweep"},
                 "peak_source": "measured cuBLAS DGEMM 8192^3 FP64 on this GPU (FP64 has no entry in MEASURED_PEAKS.json)",
@@ -494,11 +516,12 @@ def run_gpu(args):
         config = {"workload": wl_desc, "chains_per_gpu": n}
         if metric_wl:
             config.update(CFG)
-        config.update({"expk_mode": modes[0] if len(modes) == 1 else modes,
+        config.update({"sweep_mode": sweep_mode, "expk_mode": modes[0] if len(modes) == 1 else modes,
                        "delay_depth": depths[0] if len(depths) == 1 else depths, "cuda_graph": True,
                        "thermalization_sweeps": args.thermalize,
-                       "autotune": [{"nl": t["nl"], "expk": "separable" if t["expk_mode"] == 1 else "dense",
+                       "autotune": [{"nl": t["nl"], "expk": {1: "separable", 0: "dense"}.get(t["expk_mode"], "-"),
                                      "k": t["delay_depth"], "cluster": t["cluster_size"],
+                                     "sweep": "persistent" if t["sweep_mode"] == hq.SWEEP_PERSISTENT else "launches",
                                      "ms_per_sweep": round(t["ms_per_sweep"], 3), "chosen": t["chosen"]} for t in tune],
                        "l2": "working set per GPU of chain state far above the 126 MB L2 (no flush needed)"})
         line = {

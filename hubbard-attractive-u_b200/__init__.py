@@ -7,8 +7,8 @@ reference's configuration and measurement schedule.
 """
 from .capi import (Engine, HqError, lib, EXPORTS, SWEEP_UP, SWEEP_DOWN, SWEEP_DYNAMIC, SWEEP_MEASURE,
                    SWEEP_SNAPSHOT, SWEEP_LOG_RATIOS, G_CURRENT, G_TT, G_T0, G_0T, EXPK_DENSE,
-                   EXPK_SEPARABLE, EXPK_AUTO)
+                   EXPK_SEPARABLE, EXPK_AUTO, SWEEP_LAUNCHES, SWEEP_PERSISTENT)
 
 __all__ = ["Engine", "HqError", "lib", "EXPORTS", "SWEEP_UP", "SWEEP_DOWN", "SWEEP_DYNAMIC", "SWEEP_MEASURE",
            "SWEEP_SNAPSHOT", "SWEEP_LOG_RATIOS", "G_CURRENT", "G_TT", "G_T0", "G_0T", "EXPK_DENSE",
-           "EXPK_SEPARABLE", "EXPK_AUTO"]
+           "EXPK_SEPARABLE", "EXPK_AUTO", "SWEEP_LAUNCHES", "SWEEP_PERSISTENT"]

@@ -14,8 +14,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "libhubbard_b200.so")
-SOURCES = ["hq_interval.cu", "hq_interval_cluster.cu", "hq_udt.cu", "hq_invert.cu", "hq_gemm.cu", "hq_kernels.cu", "hq_engine.cu"]
-HEADERS = ["hq_types.h", "hq_device.cuh", "hq_common.cuh", "hq_metropolis.cuh", "hq_kernels.h"]
+SOURCES = ["hq_sweep.cu", "hq_interval.cu", "hq_interval_cluster.cu", "hq_udt.cu", "hq_invert.cu", "hq_gemm.cu",
+           "hq_kernels.cu", "hq_engine.cu"]
+HEADERS = ["hq_types.h", "hq_device.cuh", "hq_common.cuh", "hq_metropolis.cuh", "hq_kernels.h", "hq_interval.cuh",
+           "hq_udt.cuh", "hq_invert.cuh", "hq_phases.cuh", "hq_cta_gemm.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 

@@ -27,8 +27,14 @@ EXPORTS = [
     "hq_ratio_log", "hq_logdet_adjoint", "hq_capture_graph", "hq_launch_graph", "hq_get_config",
     "hq_upload_fields_i8", "hq_download_fields_i8", "hq_get_stream", "hq_profile_enable", "hq_profile_collect",
     "hq_equaltime_g_noalloc", "hq_autotune", "hq_get_stack", "hq_get_rng_state", "hq_set_rng_state",
+    "hq_set_sweep_mode", "hq_get_sweep_mode", "hq_phase_cycles",
 ]
-PROFILE_CLASSES = ["interval", "bchain", "udt", "gemm", "invert", "measure", "dynamic", "adjoint", "interval_cluster"]
+PROFILE_CLASSES = ["interval", "bchain", "udt", "gemm", "invert", "measure", "dynamic", "adjoint", "interval_cluster",
+                   "sweep"]
+SWEEP_LAUNCHES, SWEEP_PERSISTENT = 0, 1
+SWEEP_PHASE_CLOCKS = 8
+PHASES = ["wait", "interval", "bchain", "udt", "push_gemm", "builder_gemm_12", "invert", "builder_gemm_34", "measure",
+          "items"]
 
 
 class HqChainParams(ctypes.Structure):
@@ -56,6 +62,7 @@ class HqTuneEntry(ctypes.Structure):
         ("ms_per_sweep", ctypes.c_double),
         ("chosen", ctypes.c_int),
         ("cluster_size", ctypes.c_int),
+        ("sweep_mode", ctypes.c_int),
     ]
 
 
@@ -110,6 +117,9 @@ def lib():
             "hq_get_stack": [vp, c_int, c_int, ip, dp, dp, dp],
             "hq_get_rng_state": [vp, c_int, ctypes.POINTER(ctypes.c_uint)],
             "hq_set_rng_state": [vp, c_int, ctypes.c_uint],
+            "hq_set_sweep_mode": [vp, c_int],
+            "hq_get_sweep_mode": [vp, ip],
+            "hq_phase_cycles": [vp, ctypes.POINTER(ctypes.c_ulonglong), c_int, c_int],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -264,16 +274,33 @@ class Engine:
         check(lib().hq_get_config(self.h, chain, ctypes.byref(m), ctypes.byref(k)))
         return m.value, k.value
 
+    def set_sweep_mode(self, mode):
+        """SWEEP_PERSISTENT (one persistent launch per sweep) or SWEEP_LAUNCHES (one launch per
+        phase and interval); drops the captured sweep graphs."""
+        check(lib().hq_set_sweep_mode(self.h, int(mode)))
+
+    def phase_cycles(self, reset=False):
+        """Cycles per phase of the persistent sweeps run with SWEEP_PHASE_CLOCKS (dict over PHASES)."""
+        buf = (ctypes.c_ulonglong * len(PHASES))()
+        check(lib().hq_phase_cycles(self.h, buf, len(PHASES), int(reset)))
+        return dict(zip(PHASES, (int(v) for v in buf)))
+
+    def sweep_mode(self):
+        m = ctypes.c_int(0)
+        check(lib().hq_get_sweep_mode(self.h, ctypes.byref(m)))
+        return m.value
+
     def autotune(self, sweeps=2):
         """Times every (expK mode, delay depth) candidate per lattice size on whole sweeps and
-        keeps the fastest; the chains' state is restored after each candidate. Returns the
-        timed candidates as dicts."""
+        keeps the fastest, then the two sweep modes (entries with nl = 0); the chains' state is
+        restored after each candidate. Returns the timed candidates as dicts."""
         cap = 64
         buf = (HqTuneEntry * cap)()
         n = ctypes.c_int(0)
         check(lib().hq_autotune(self.h, int(sweeps), buf, cap, ctypes.byref(n)))
         return [dict(nl=e.nl, expk_mode=e.expk_mode, delay_depth=e.delay_depth, ms_per_sweep=e.ms_per_sweep,
-                     chosen=bool(e.chosen), cluster_size=e.cluster_size) for e in buf[:min(n.value, cap)]]
+                     chosen=bool(e.chosen), cluster_size=e.cluster_size, sweep_mode=e.sweep_mode)
+                for e in buf[:min(n.value, cap)]]
 
     def stack(self, chain, side):
         """(length, U, D, V) of the top of a chain's left (0) or right (1) UDV stack; the

@@ -130,18 +130,19 @@ __device__ __forceinline__ bool bulk_columns_ok(const double* gsrc, int N, int l
 
 // Loads an N x N column-major matrix into shared memory (leading dimension ldd) by one bulk copy
 // per column, issued by warp 0 and completed on `bar` (initialised for one arrival, phase 0).
-// Every thread waits; on a wait that runs out the chain's status word is set. The caller has
-// checked bulk_columns_ok. A barrier must separate mbar_init from this call.
+// Every thread waits for phase `parity` of the barrier (its uses so far, mod 2); on a wait that
+// runs out the chain's status word is set. The caller has checked bulk_columns_ok. A barrier
+// must separate mbar_init from this call.
 __device__ __forceinline__ void load_mat_bulk(double* dst, int ldd, const double* src, int N, uint64_t* bar,
-                                              double* status) {
+                                              double* status, unsigned parity = 0) {
   const unsigned col = static_cast<unsigned>(N) * sizeof(double);
   if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, col * static_cast<unsigned>(N));
   __syncwarp();
   if (threadIdx.x < 32)
     for (int j = threadIdx.x; j < N; j += 32) bulk_g2s(dst + (size_t)j * ldd, src + (size_t)j * N, col, bar);
-  if (!mbar_wait_bounded(bar, 0)) {
+  if (!mbar_wait_bounded(bar, parity)) {
     if (threadIdx.x == 0) *status = 1.0;
-    mbar_wait_bounded(bar, 0);  // the copies in flight still land in this CTA's shared memory
+    mbar_wait_bounded(bar, parity);  // the copies in flight still land in this CTA's shared memory
   }
 }
 

@@ -193,6 +193,18 @@ struct hq_ctx {
   // the chains and stream the launch helpers currently issue for (default: all, main stream)
   int cur_c0 = 0, cur_n = 0;
   cudaStream_t cur_st = nullptr;
+  // persistent sweep (HQ_SWEEP_PERSISTENT): per chain {n_stab, cost of an interval}, the total
+  // of the chains' intervals, the per-chain builder job lists of every (direction, interval,
+  // phase), the counter / progress / claim words
+  bool sweep_capable = false;
+  int sweep_mode = HQ_SWEEP_LAUNCHES;
+  int2* d_items = nullptr;
+  int nitems = 0;
+  const HqGemmJob** d_lists = nullptr;
+  int* d_ctl = nullptr;
+  int nctl = 0;
+  unsigned long long* d_clk = nullptr;  // phase cycles (HQ_SWEEP_PHASE_CLOCKS)
+  int sweep_grid = 0;
   bool at_zero = false;         // stacks at tau = 0 (left empty, right full)
   bool at_beta = false;         // stacks at tau = beta
   bool initialised = false;
@@ -200,6 +212,10 @@ struct hq_ctx {
   ~hq_ctx() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
     if (d_jobs) cudaFree(d_jobs);
+    if (d_items) cudaFree(d_items);
+    if (d_lists) cudaFree(d_lists);
+    if (d_ctl) cudaFree(d_ctl);
+    if (d_clk) cudaFree(d_clk);
     if (d_desc) cudaFree(d_desc);
     if (d_acc_all) cudaFree(d_acc_all);
     if (h_acc_all) cudaFreeHost(h_acc_all);
@@ -369,8 +385,55 @@ void build_jobs(hq_ctx* c) {
   }
 }
 
+// The persistent sweep's scheduling data: per chain {n_stab, estimated cycles of one interval}
+// (the kernel claims, among the ready chains, the one with the longest remaining work); the
+// per-chain job lists of the five builder phases of every (direction, interval); the counter,
+// progress and claim words; the grid (as many CTAs as are resident at once).
+int item_cost(const ChainHost& h) {
+  // thousands of cycles of one interval, of the measured shape: wrap, flushes, factorisations
+  // and products ~ N^3, the walk, reflectors and pivots ~ N sequential steps
+  const double N = h.N, pace = h.p.stabilization_pace;
+  return int(1e-3 * (N * N * N * (0.074 * pace + 0.54)) + N * (5.0 + 0.3 * pace)) + 1;
+}
+
+void setup_sweep(hq_ctx* c) {
+  HQ_CUDA(hq::prepare_sweep(c->Nmax, c->kmax_max));
+  int sms = 0, per_sm = 0;
+  HQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  HQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hq::fn_sweep(), HQ_INT_THREADS,
+                                                        hq::smem_sweep_bytes(c->Nmax, c->kmax_max)));
+  if (per_sm < 1) return;  // not launchable here: the context keeps the launch sequence
+  c->sweep_grid = sms * per_sm;
+  std::vector<int2> cinfo(c->n);
+  c->nitems = 0;
+  for (int i = 0; i < c->n; ++i) {
+    cinfo[i] = make_int2(c->ch[i].n_stab, item_cost(c->ch[i]));
+    c->nitems += c->ch[i].n_stab;
+  }
+  std::vector<const HqGemmJob*> lists;
+  const int phases[5] = {PH_PUSH, PH_B1, PH_B2, PH_B3, PH_B4};
+  for (int dir = 0; dir < 2; ++dir)
+    for (int b = 0; b < c->nstab_max; ++b)
+      for (int ph : phases) {
+        auto it = c->jobs.find(std::make_tuple(ph, dir, b));
+        if (it == c->jobs.end() || it->second.second != c->n) throw HqError(HQ_E_INVALID, "internal: sweep job list");
+        lists.push_back(it->second.first);
+      }
+  c->nctl = int(hq::sweep_ctl_ints(c->n));
+  HQ_CUDA(cudaMalloc(&c->d_items, cinfo.size() * sizeof(int2)));
+  HQ_CUDA(cudaMalloc(&c->d_lists, lists.size() * sizeof(HqGemmJob*)));
+  HQ_CUDA(cudaMalloc(&c->d_ctl, size_t(c->nctl) * sizeof(int)));
+  HQ_CUDA(cudaMemcpy(c->d_items, cinfo.data(), cinfo.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  HQ_CUDA(cudaMemcpy(c->d_lists, lists.data(), lists.size() * sizeof(HqGemmJob*), cudaMemcpyHostToDevice));
+  HQ_CUDA(cudaMemset(c->d_ctl, 0, size_t(c->nctl) * sizeof(int)));
+  HQ_CUDA(cudaMalloc(&c->d_clk, HQ_PHASES * sizeof(unsigned long long)));
+  HQ_CUDA(cudaMemset(c->d_clk, 0, HQ_PHASES * sizeof(unsigned long long)));
+  c->sweep_capable = true;
+}
+
 // launch classes of the per-launch timing (hq_profile_collect)
-enum ProfClass { PC_INTERVAL = 0, PC_BCHAIN, PC_UDT, PC_GEMM, PC_INVERT, PC_MEASURE, PC_DYN, PC_ADJ, PC_INTERVAL_CL, PC_COUNT };
+enum ProfClass { PC_INTERVAL = 0, PC_BCHAIN, PC_UDT, PC_GEMM, PC_INVERT, PC_MEASURE, PC_DYN, PC_ADJ, PC_INTERVAL_CL,
+                 PC_SWEEP, PC_COUNT };
 
 struct ProfScope {
   hq_ctx* c;
@@ -497,6 +560,13 @@ void in_groups(hq_ctx* c, F&& body) {
 void issue_sweep(hq_ctx* c, int dir, int flags) {
   c->prof_next = 0;
   const int kf = flags & (HQ_F_MEASURE | HQ_F_SNAPSHOT | HQ_F_LOG_RATIOS);
+  if ((dir == HQ_UP || dir == HQ_DOWN) && c->sweep_mode == HQ_SWEEP_PERSISTENT) {
+    ProfScope ps(c, PC_SWEEP);
+    HQ_CUDA(hq::launch_sweep(c->d_desc, c->n, c->d_items, c->nitems, c->d_lists, c->nstab_max, dir,
+                             kf | (flags & HQ_F_PHASE_CLOCKS), c->d_ctl, c->d_clk, c->sweep_grid, c->Nmax,
+                             c->kmax_max, c->stream));
+    return;
+  }
   if (dir == HQ_UP || dir == HQ_DOWN) {
     in_groups(c, [&] {
       const Cur gr = cur(c);
@@ -791,6 +861,13 @@ int hq_create(int device, int n_chains, const hq_chain_params* params, hq_ctx** 
   HQ_CUDA(cudaMallocHost(&c->h_acc_all, size_t(c->n) * HQ_ACC_COUNT * sizeof(double)));
   upload_desc(c.get());
   build_jobs(c.get());
+  if (c->resident && hq::sweep_fits(c->Nmax, c->kmax_max, optin)) {
+    setup_sweep(c.get());
+    // HQ_SWEEP_MODE=persistent | launches overrides the default mode (for comparisons)
+    const char* m = std::getenv("HQ_SWEEP_MODE");
+    if (m && std::strcmp(m, "persistent") == 0) c->sweep_mode = HQ_SWEEP_PERSISTENT;
+    if (m && std::strcmp(m, "launches") == 0) c->sweep_mode = HQ_SWEEP_LAUNCHES;
+  }
   HQ_CUDA(cudaStreamSynchronize(c->stream));
   *out = c.release();
   HQ_API_END
@@ -1208,6 +1285,37 @@ int hq_get_config(hq_ctx* c, int chain, int* expk_mode, int* delay_depth) {
 // reference's SvdStack::MatrixU / SingularValues / MatrixV (include/utils/svd_stack.hpp:83-103).
 // Between whole sweeps the stacks are either at tau = 0 (left empty, right full) or at
 // tau = beta (left full, right empty).
+int hq_set_sweep_mode(hq_ctx* c, int mode) {
+  HQ_API_BEGIN
+  if (!c) throw HqError(HQ_E_INVALID, "null context");
+  if (mode != HQ_SWEEP_LAUNCHES && mode != HQ_SWEEP_PERSISTENT) throw HqError(HQ_E_INVALID, "unknown sweep mode");
+  if (mode == HQ_SWEEP_PERSISTENT && !c->sweep_capable)
+    throw HqError(HQ_E_RANGE, "persistent sweep: the chains' matrices do not fit in one SM's shared memory");
+  HQ_CUDA(cudaStreamSynchronize(c->stream));
+  c->sweep_mode = mode;
+  for (auto& g : c->graphs) cudaGraphExecDestroy(g.second);
+  c->graphs.clear();
+  HQ_API_END
+}
+
+int hq_phase_cycles(hq_ctx* c, unsigned long long* out, int n, int reset) {
+  HQ_API_BEGIN
+  if (!c || (n > 0 && !out)) throw HqError(HQ_E_INVALID, "null argument");
+  HQ_CUDA(cudaStreamSynchronize(c->stream));
+  unsigned long long h[HQ_PHASES] = {};
+  if (c->d_clk) HQ_CUDA(cudaMemcpy(h, c->d_clk, sizeof(h), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < n && k < HQ_PHASES; ++k) out[k] = h[k];
+  if (reset && c->d_clk) HQ_CUDA(cudaMemset(c->d_clk, 0, sizeof(h)));
+  HQ_API_END
+}
+
+int hq_get_sweep_mode(hq_ctx* c, int* mode) {
+  HQ_API_BEGIN
+  if (!c || !mode) throw HqError(HQ_E_INVALID, "null argument");
+  *mode = c->sweep_mode;
+  HQ_API_END
+}
+
 int hq_get_stack(hq_ctx* c, int chain, int side, int* length, double* U, double* D, double* V) {
   HQ_API_BEGIN
   check_chain(c, chain);
@@ -1263,6 +1371,10 @@ int hq_autotune(hq_ctx* c, int sweeps, hq_tune_entry* entries, int capacity, int
   try {
     HQ_CUDA(cudaEventCreate(&e0));
     HQ_CUDA(cudaEventCreate(&e1));
+    // the candidates are issued directly: a captured sweep would keep its capture's choices
+    HQ_CUDA(cudaStreamSynchronize(c->stream));
+    for (auto& gr : c->graphs) cudaGraphExecDestroy(gr.second);
+    c->graphs.clear();
     HQ_CUDA(cudaMemcpyAsync(snap, c->arena, c->arena_bytes, cudaMemcpyDeviceToDevice, c->stream));
     for (auto& g : groups) {
       const int nl = g.first;
@@ -1298,6 +1410,7 @@ int hq_autotune(hq_ctx* c, int sweeps, hq_tune_entry* entries, int capacity, int
           hq_tune_entry t;
           t.nl = nl; t.expk_mode = mode; t.delay_depth = k; t.ms_per_sweep = double(ms) / sweeps; t.chosen = 0;
           t.cluster_size = cl;
+          t.sweep_mode = c->sweep_mode;
           if (t.ms_per_sweep < best) { best = t.ms_per_sweep; best_at = out.size(); }
           out.push_back(t);
         }
@@ -1311,6 +1424,29 @@ int hq_autotune(hq_ctx* c, int sweeps, hq_tune_entry* entries, int capacity, int
       }
     }
     upload_desc(c);
+    // the sweep mode for the whole context with the per-size choices made above
+    if (c->sweep_capable) {
+      double best = 1e300;
+      size_t best_at = out.size();
+      for (int m : {HQ_SWEEP_LAUNCHES, HQ_SWEEP_PERSISTENT}) {
+        c->sweep_mode = m;
+        run(1);  // warm-up
+        HQ_CUDA(cudaEventRecord(e0, c->stream));
+        run(sweeps);
+        HQ_CUDA(cudaEventRecord(e1, c->stream));
+        HQ_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        HQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        restore();
+        hq_tune_entry t;
+        t.nl = 0; t.expk_mode = -1; t.delay_depth = 0; t.cluster_size = 0; t.sweep_mode = m; t.chosen = 0;
+        t.ms_per_sweep = double(ms) / sweeps;
+        if (t.ms_per_sweep < best) { best = t.ms_per_sweep; best_at = out.size(); }
+        out.push_back(t);
+      }
+      out[best_at].chosen = 1;
+      c->sweep_mode = out[best_at].sweep_mode;
+    }
     HQ_CUDA(cudaStreamSynchronize(c->stream));
     // captured sweeps hold the kernel choice of their capture
     for (auto& gr : c->graphs) cudaGraphExecDestroy(gr.second);

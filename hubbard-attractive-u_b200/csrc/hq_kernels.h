@@ -44,6 +44,20 @@ cudaError_t prepare_interval_cl();
 size_t smem_bchain_cols_bytes();
 cudaError_t launch_bchain_cols(const HqChain* chains, int n, int dir, int b, cudaStream_t st);
 const void* fn_bchain_cols();
+// the persistent sweep kernel: one launch per up / down sweep, one CTA per SM taking items (the
+// next interval of one chain) by longest remaining work (cinfo[c] = {n_stab, cost per interval};
+// nitems = the sum of n_stab); lists[(dir * nstab_max + b) * 5 + phase] is the per-chain job list
+// of builder phase PH_PUSH..PH_B4; ctl holds sweep_ctl_ints(nchains) ints (counters, progress and
+// claim words), zeroed by the launch; clk receives the phase cycles when flags has
+// HQ_F_PHASE_CLOCKS
+size_t smem_sweep_bytes(int Nmax, int kmax);
+size_t sweep_ctl_ints(int nchains);
+bool sweep_fits(int Nmax, int kmax, size_t optin);
+cudaError_t prepare_sweep(int Nmax, int kmax);
+cudaError_t launch_sweep(const HqChain* chains, int nchains, const int2* cinfo, int nitems,
+                         const HqGemmJob* const* lists, int nstab_max, int dir, int flags, int* ctl,
+                         unsigned long long* clk, int grid, int Nmax, int kmax, cudaStream_t st);
+const void* fn_sweep();
 cudaError_t launch_adj_interval(const HqChain* chains, int n, int b, int Nmax, bool resident, cudaStream_t st);
 cudaError_t launch_adj_last(const HqChain* chains, int n, int b, cudaStream_t st);
 }  // namespace hq

@@ -23,6 +23,7 @@ enum HqFlags {
   HQ_F_MEASURE = 1,        // accumulate fused equal-time estimators
   HQ_F_SNAPSHOT = 2,       // store G(tau,tau) per slice (the reference's vecgftt)
   HQ_F_LOG_RATIOS = 4,     // store every acceptance ratio (replay checks)
+  HQ_F_PHASE_CLOCKS = 8,   // persistent sweep: accumulate the clock64 cycles of every phase
 };
 
 // per-chain accumulators (doubles), laid out at HqChain::acc

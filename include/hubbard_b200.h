@@ -47,6 +47,7 @@ extern "C" {
 #define HQ_SWEEP_MEASURE 1  /* accumulate the equal-time estimators (filling, double occupancy, s-wave) */
 #define HQ_SWEEP_SNAPSHOT 2 /* keep G(tau,tau) of every slice (the reference's vecgftt) */
 #define HQ_SWEEP_LOG_RATIOS 4 /* record every Metropolis acceptance ratio (replay checks) */
+#define HQ_SWEEP_PHASE_CLOCKS 8 /* persistent sweep: count the cycles of every phase (hq_phase_cycles) */
 
 /* Green's function selectors for hq_get_g (include/dqmc_core.h:76-81) */
 #define HQ_G_CURRENT 0 /* current_gftt() */
@@ -167,12 +168,40 @@ HQ_API int hq_get_stream(hq_ctx* ctx, void** stream);
  * every launch of the most recent sweep to ms[class] and 1 to counts[class]. Classes:
  * 0 interval (wrap + Metropolis), 1 B chain, 2 UDV factorisation, 3 batched GEMM,
  * 4 inversion, 5 boundary measurement, 6 displaced propagation, 7 log-det adjoint,
- * 8 interval on four-CTA clusters (16 x 16 lattices, G in distributed shared memory). */
+ * 8 interval on four-CTA clusters (16 x 16 lattices, G in distributed shared memory),
+ * 9 persistent sweep (HQ_SWEEP_PERSISTENT: every phase of every chain in one launch). */
 HQ_API int hq_profile_enable(hq_ctx* ctx, int on);
 HQ_API int hq_profile_collect(hq_ctx* ctx, double* ms, long long* counts, int nclasses);
 
 /* Per-chain expK mode and delay depth actually in use (after autotuning). */
 HQ_API int hq_get_config(hq_ctx* ctx, int chain, int* expk_mode, int* delay_depth);
+
+/* How an up or down sweep is issued (no counterpart in the reference, which updates one chain
+ * per MPI rank; this is the batched form of DQMC::Core::sweep_from_0_to_beta /
+ * sweep_from_beta_to_0, src/dqmc_core.cpp:167-284):
+ *  HQ_SWEEP_LAUNCHES   one kernel launch per phase and stabilisation interval (wrap +
+ *                      Metropolis, B chain, UDV, GEMMs, inverse, measurement), the chains split
+ *                      into groups on forked streams;
+ *  HQ_SWEEP_PERSISTENT one persistent launch per sweep: one CTA per SM takes (chain, interval)
+ *                      items from a device queue and runs all the phases of an item; the
+ *                      chains' intervals follow each other through device-side progress words.
+ * Both give the same G and field trajectories. PERSISTENT needs every chain's matrices to fit
+ * in one SM's shared memory (N <= 144 on B200); hq_set_sweep_mode returns HQ_E_RANGE
+ * otherwise. Setting a mode drops the captured sweep graphs. hq_autotune picks the faster. */
+#define HQ_SWEEP_LAUNCHES 0
+#define HQ_SWEEP_PERSISTENT 1
+HQ_API int hq_set_sweep_mode(hq_ctx* ctx, int mode);
+HQ_API int hq_get_sweep_mode(hq_ctx* ctx, int* mode);
+
+/* Phase cycles of the persistent sweep: for sweeps run with HQ_SWEEP_PHASE_CLOCKS in the
+ * persistent mode, the clock64 cycles that the SM running an item spent in each phase, summed
+ * over all items since the last reset (no counterpart in the reference; a profiling aid).
+ * out[0] waiting for the chain's previous interval, [1] wrap + Metropolis, [2] B chain,
+ * [3] UDV factorisation, [4] cumulative V^T, [5] builder products 1-2, [6] inverse,
+ * [7] builder products 3-4, [8] measurement, [9] items. Writes min(n, 10) entries; reset != 0
+ * zeroes the counters afterwards. Waits for the context stream. */
+#define HQ_PHASES 10
+HQ_API int hq_phase_cycles(hq_ctx* ctx, unsigned long long* out, int n, int reset);
 
 /* Top of a chain's UDV stack (side 0: left, 1: right), replacing Utils::SvdStack's
  * StackLength / MatrixU / SingularValues / MatrixV (include/utils/svd_stack.hpp:78-103):
@@ -197,13 +226,16 @@ typedef struct {
   double ms_per_sweep; /* device time of one directional sweep of the whole context */
   int chosen;          /* 1: the candidate now in use for this lattice size */
   int cluster_size;    /* CTAs per chain of the interval kernel: 4 (G in a cluster's shared memory) or 1 */
+  int sweep_mode;      /* HQ_SWEEP_LAUNCHES or HQ_SWEEP_PERSISTENT; nl = 0 marks the entries that
+                          time the two modes for the whole context after the per-size choices */
 } hq_tune_entry;
 
 /* Picks, per lattice size, the expK application (the is_fft choice of the reference's
  * config, src/hubbard.cpp:38-80, here separable circulant passes vs dense DMMA GEMM), the
  * delay depth and, for the 16 x 16 lattice, the cluster size of the interval kernel (four
  * CTAs with G in distributed shared memory, or one CTA with G in global memory) by timing
- * `sweeps` directional sweeps of the whole context per candidate. The device state is
+ * `sweeps` directional sweeps of the whole context per candidate; then, where the context can
+ * run it, the sweep mode (HQ_SWEEP_PERSISTENT or HQ_SWEEP_LAUNCHES) the same way. The device state is
  * restored after each candidate: the Markov chains are unaffected. Captured sweep graphs are
  * dropped (recapture them). Needs hq_init_stacks_and_g; allocates one temporary copy of the
  * context's device state. Writes up to `capacity` entries and the total count to *n_entries. */

@@ -37,6 +37,13 @@ class Context {
     ctx_.reset(c, [](hq_ctx* p) { hq_destroy(p); });
   }
   hq_ctx* get() const { return ctx_.get(); }
+  // HQ_SWEEP_PERSISTENT (one launch per sweep) or HQ_SWEEP_LAUNCHES (one per phase and interval)
+  void set_sweep_mode(int mode) { check(hq_set_sweep_mode(get(), mode)); }
+  int sweep_mode() const {
+    int m = 0;
+    check(hq_get_sweep_mode(get(), &m));
+    return m;
+  }
 
  private:
   std::shared_ptr<hq_ctx> ctx_;

@@ -28,6 +28,12 @@ def test_autotune_picks_the_fastest_and_leaves_the_chains_unchanged(hq):
         assert best["chosen"] and best["ms_per_sweep"] > 0.0
         for c in chains:
             assert a.config(c) == (best["expk_mode"], best["delay_depth"])
+    # then the two sweep modes for the whole context (nl = 0); the faster one is in use
+    modes = [t for t in table if t["nl"] == 0]
+    assert sorted(t["sweep_mode"] for t in modes) == [hq.SWEEP_LAUNCHES, hq.SWEEP_PERSISTENT]
+    assert sum(t["chosen"] for t in modes) == 1
+    fastest = min(modes, key=lambda t: t["ms_per_sweep"])
+    assert fastest["chosen"] and a.sweep_mode() == fastest["sweep_mode"]
     # the tuning sweeps were undone: both engines follow the same trajectory
     for d in (UP, DOWN, UP):
         a.sweep(d, hq.SWEEP_MEASURE)
@@ -64,6 +70,8 @@ def test_autotune_chooses_the_cluster_size_of_16x16_chains(hq):
     clustered = [t for t in table if t["cluster_size"] == 4]
     assert len(clustered) == 1 and clustered[0]["expk_mode"] == hq.EXPK_SEPARABLE and clustered[0]["delay_depth"] == 16
     assert len([t for t in table if t["cluster_size"] == 1]) == 6
+    # 16 x 16 chains do not fit one SM: no sweep-mode entries, the launch sequence stays
+    assert not [t for t in table if t["nl"] == 0] and a.sweep_mode() == hq.SWEEP_LAUNCHES
     assert sum(t["chosen"] for t in table) == 1
     best = min(table, key=lambda t: t["ms_per_sweep"])
     assert best["chosen"]

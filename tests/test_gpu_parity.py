@@ -329,8 +329,10 @@ def test_c5_lattice_on_the_non_resident_path(hq, oracle):
 
 
 def test_profiling_with_and_without_graphs(hq):
-    """Per-launch device times (hq_profile_collect) of a plain sweep and of a graph replay."""
+    """Per-launch device times (hq_profile_collect) of a plain sweep and of a graph replay, in
+    the launch-sequence mode (one interval launch per stabilisation interval)."""
     e = hq.Engine([dict(nl=4, u=4.0, beta=4.0, nt=40, stabilization_pace=10, seed=2)])
+    e.set_sweep_mode(hq.SWEEP_LAUNCHES)
     e.fields_random()
     e.init()
     e.profile_enable(True)
