@@ -9,14 +9,14 @@ namespace hq {
 //  One-CTA GEMM of a builder job (the semantics of k_gemm: C = alpha op(A) diag(ks) op(B)
 //  with row / column scalings, beta and the wrap-error epilogue). The output is cut into
 //  16 x 24 blocks (three 16 x 8 DMMA tiles); warp w accumulates blocks w, w + 8, ... over
-//  all of K, which streams through shared memory in chunks of 16 (cp.async, double
-//  buffered). Each output element sees the DMMA steps in increasing k, as in k_gemm, so the
+//  all of K, which streams through shared memory in chunks of 16 (cp.async, kCtaStages
+//  buffers). Each output element sees the DMMA steps in increasing k, as in k_gemm, so the
 //  two agree bitwise. Shared layouts (conflict-free fragment loads):
 //    op(X) contiguous along k : sX[r * 20 + k]      otherwise : sX[k * ldr + r], ldr = 4 (mod 16)
 // ---------------------------------------------------------------------------------
 constexpr int kCtaKc = 16, kCtaLdk = 20, kCtaMaxB = 7;
 #ifndef HQ_CTA_KK_UNROLL
-#define HQ_CTA_KK_UNROLL 1
+#define HQ_CTA_KK_UNROLL 4
 #endif
 constexpr int kCtaKkUnroll = HQ_CTA_KK_UNROLL;
 
@@ -25,10 +25,12 @@ __host__ __device__ constexpr inline int cta_pad24(int x) { return ((x + 23) / 2
 __host__ __device__ constexpr inline int cta_stage_doubles(int R) {
   return (kCtaKc * panel_ld(R) > R * kCtaLdk) ? kCtaKc * panel_ld(R) : R * kCtaLdk;
 }
-// doubles of shared memory of gemm_cta for M x Nc outputs: two stages of both operands, the
-// k-scalings of two chunks and the row / column scalings of the output
+// chunks of K in flight: three stages hide the latency of operands that come from HBM
+constexpr int kCtaStages = 3;
+// doubles of shared memory of gemm_cta for M x Nc outputs: the stages of both operands, the
+// k-scalings of as many chunks and the row / column scalings of the output
 __host__ __device__ constexpr inline size_t cta_gemm_doubles(int M, int Nc) {
-  return 2 * (size_t)cta_stage_doubles(cta_pad16(M)) + 2 * (size_t)cta_stage_doubles(cta_pad24(Nc)) + 2 * kCtaKc +
+  return kCtaStages * ((size_t)cta_stage_doubles(cta_pad16(M)) + (size_t)cta_stage_doubles(cta_pad24(Nc)) + kCtaKc) +
          cta_pad16(M) + cta_pad24(Nc);
 }
 
@@ -78,11 +80,19 @@ __device__ __forceinline__ void cta_stage8(const double* X, int ldx, bool kmaj, 
 }
 
 // C of job `job` for one transpose case (AMAJ: op(A) = A^T, contiguous along k; BMAJ: op(B) = B,
-// contiguous along k). Not inlined: its registers are allocated apart from the other phases of
-// the persistent kernel. `smem` holds cta_gemm_doubles(M, Nc) doubles, red >= 32 doubles. Every
-// thread calls it.
+// contiguous along k; KS: k-scalings). Inlined by default (HQ_CTA_NOINLINE=1 makes it a call):
+// measured 5-15% faster per product. `smem` holds cta_gemm_doubles(M, Nc) doubles, red >= 32
+// doubles. Every thread calls it.
+#ifndef HQ_CTA_NOINLINE
+#define HQ_CTA_NOINLINE 0
+#endif
+#if HQ_CTA_NOINLINE
+#define HQ_CTA_FN_ATTR __noinline__
+#else
+#define HQ_CTA_FN_ATTR __forceinline__
+#endif
 template <bool AMAJ, bool BMAJ, bool KS>
-__device__ __noinline__ void gemm_cta_t(const HqGemmJob& job, double* smem, double* red) {
+__device__ HQ_CTA_FN_ATTR void gemm_cta_t(const HqGemmJob& job, double* smem, double* red) {
   const double* __restrict__ Ag = job.A;
   const double* __restrict__ Bg = job.B;
   double* Cg = job.C;
@@ -97,9 +107,9 @@ __device__ __noinline__ void gemm_cta_t(const HqGemmJob& job, double* smem, doub
   const int ldA = panel_ld(Mp), ldB = panel_ld(Np);
   const int SA = cta_stage_doubles(Mp), SB = cta_stage_doubles(Np);
   double* sA0 = smem;
-  double* sB0 = smem + 2 * (size_t)SA;
-  double* sK0 = sB0 + 2 * (size_t)SB;
-  double* sR = sK0 + 2 * kCtaKc;  // row scalings of the output
+  double* sB0 = smem + kCtaStages * (size_t)SA;
+  double* sK0 = sB0 + kCtaStages * (size_t)SB;
+  double* sR = sK0 + kCtaStages * kCtaKc;  // row scalings of the output
   double* sC = sR + Mp;           // column scalings
   const bool pa = (lda % 2 == 0) && ((reinterpret_cast<uintptr_t>(Ag) & 15) == 0);
   const bool pb = (ldb % 2 == 0) && ((reinterpret_cast<uintptr_t>(Bg) & 15) == 0);
@@ -133,25 +143,27 @@ __device__ __noinline__ void gemm_cta_t(const HqGemmJob& job, double* smem, doub
 #pragma unroll
       for (int j = 0; j < 3; ++j) acc[i][j][0] = acc[i][j][1] = acc[i][j][2] = acc[i][j][3] = 0.0;
     __syncthreads();  // the stage buffers are free
-    stage(0, 0);
-    if (threadIdx.x < kCtaKc) sK0[threadIdx.x] = ((int)threadIdx.x < K) ? vscale(ks, ks_mode, threadIdx.x) : 0.0;
-    cp_async_commit();
-    for (int c = 0; c < nchunks; ++c) {
-      const int cur = c & 1;
-      if (c + 1 < nchunks) {
-        const int k1 = (c + 1) * kCtaKc;
-        stage(k1, cur ^ 1);
+    // chunk c lives in stage c mod kCtaStages; chunks c + 1 .. c + kCtaStages - 1 are in flight
+    // while chunk c is multiplied
+    auto stage_chunk = [&](int cc) {
+      if (cc < nchunks) {
+        const int k1 = cc * kCtaKc, buf = cc % kCtaStages;
+        stage(k1, buf);
         if (threadIdx.x < kCtaKc)
-          sK0[(cur ^ 1) * kCtaKc + threadIdx.x] = (k1 + (int)threadIdx.x < K) ? vscale(ks, ks_mode, k1 + threadIdx.x) : 0.0;
+          sK0[buf * kCtaKc + threadIdx.x] = (k1 + (int)threadIdx.x < K) ? vscale(ks, ks_mode, k1 + threadIdx.x) : 0.0;
       }
       cp_async_commit();
-      cp_async_wait<1>();
+    };
+#pragma unroll
+    for (int cc = 0; cc < kCtaStages - 1; ++cc) stage_chunk(cc);
+    for (int c = 0; c < nchunks; ++c) {
+      const int cur = c % kCtaStages;
+      stage_chunk(c + kCtaStages - 1);
+      cp_async_wait<kCtaStages - 1>();
       __syncthreads();
       const double* A_ = sA0 + cur * (size_t)SA;
       const double* B_ = sB0 + cur * (size_t)SB;
       const double* K_ = sK0 + cur * kCtaKc;
-      // the k-steps of a chunk stay a loop: unrolled, the body outgrows the instruction cache
-      // (measured: instruction-fetch stalls, tensor pipe active 34% instead of 71%)
 #pragma unroll kCtaKkUnroll
       for (int kk = 0; kk < kCtaKc; kk += 4) {
         const int k = kk + q;

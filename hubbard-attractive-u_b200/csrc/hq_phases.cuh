@@ -17,8 +17,11 @@ namespace hq {
 // ---------------------------------------------------------------------------------
 // The B products of interval b applied to the top of the pushing stack (X = U_top D_top, or 1),
 // into ch.X. `smem` is the dynamic region (N x smem_ld(N) when resident, then the stage); s holds
-// N fields (shared). Every thread of the block calls it; the chain is active and b < n_stab.
-__device__ __forceinline__ void bchain_body(const HqChain& ch, int dir, int b, bool resident, double* smem, int8_t* s) {
+// N fields (shared). keep_x (resident only): X stays at the start of `smem` (leading dimension
+// smem_ld(N)) for the factorisation that follows in the same block, instead of going to ch.X.
+// Every thread of the block calls it; the chain is active and b < n_stab.
+__device__ __forceinline__ void bchain_body(const HqChain& ch, int dir, int b, bool resident, double* smem, int8_t* s,
+                                            bool keep_x = false) {
   const int N = ch.N;
   int t_lo, t_hi;
   interval_range(ch.nt, ch.pace, ch.n_stab, dir, b, t_lo, t_hi);
@@ -65,7 +68,7 @@ __device__ __forceinline__ void bchain_body(const HqChain& ch, int dir, int b, b
       __syncthreads();
     }
   }
-  if (resident) copy_mat(ch.X, N, X, ld, N);
+  if (resident && !keep_x) copy_mat(ch.X, N, X, ld, N);
 }
 
 // ---------------------------------------------------------------------------------

@@ -74,15 +74,19 @@ __device__ int2 take_item(const int2* __restrict__ cinfo, int nchains, int nitem
   for (int look = 0; look < kSweepWaitLimit; ++look) {
     if (ld_relaxed(ctl + 1) != 0) return make_int2(-2, 0);
     if (ld_relaxed(ctl) >= nitems) return make_int2(-1, 0);
-    // this lane's ready chain of the largest remaining work (ties: the lower index)
+    // this lane's ready chain of the largest remaining work; among equals each CTA prefers the
+    // chains from its own offset on (rank (c - rot) mod n), so that CTAs looking at the same time
+    // claim different chains of equal work instead of contending for one
+    const int rot = (int)(((long long)blockIdx.x * nchains) / gridDim.x);
     long long key = -1;
-    int bc = -1, bb = 0;
+    int bc = -1, bb = 0, br = 0;
     for (int c = lane; c < nchains; c += 32) {
       const int2 ci = cinfo[c];
       const int nb = ld_relaxed(next + c);
       if (nb < ci.x && ld_acquire(progress + c) == nb) {
         const long long k = (long long)(ci.x - nb) * ci.y;
-        if (k > key) { key = k; bc = c; bb = nb; }
+        const int r = c >= rot ? c - rot : c - rot + nchains;
+        if (k > key || (k == key && r < br)) { key = k; bc = c; bb = nb; br = r; }
       }
     }
 #pragma unroll
@@ -90,7 +94,8 @@ __device__ int2 take_item(const int2* __restrict__ cinfo, int nchains, int nitem
       const long long ok = __shfl_xor_sync(0xffffffffu, key, o);
       const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
       const int ob = __shfl_xor_sync(0xffffffffu, bb, o);
-      if (ok > key || (ok == key && oc >= 0 && (bc < 0 || oc < bc))) { key = ok; bc = oc; bb = ob; }
+      const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+      if (ok > key || (ok == key && oc >= 0 && (bc < 0 || orr < br))) { key = ok; bc = oc; bb = ob; br = orr; }
     }
     if (bc < 0) {
       __nanosleep(256);
@@ -175,30 +180,29 @@ k_sweep(const HqChain* __restrict__ chains, int nchains, const int2* __restrict_
     }
     mark(1);
     // ---- stack push: B chain, UDV factorisation, cumulative V^T ----
-    bchain_body(ch, dir, b, true, smem, reinterpret_cast<int8_t*>(smem + bchain_doubles(N)));
+    // X = B ... B U_top D_top stays in shared memory for the factorisation
+    bchain_body(ch, dir, b, true, smem, reinterpret_cast<int8_t*>(smem + bchain_doubles(N)), true);
     __syncthreads();
     mark(2);
-    udt_body<2>(ch, side, b, true, smem, mv);
+    udt_body<2>(ch, side, b, true, smem, mv, true);
     __syncthreads();
     mark(3);
     const HqGemmJob* const* L = lists + ((size_t)dir * nstab_max + b) * 5;
-    // builder phase ph (PH_PUSH, B1, B2, B3, B4): the chain's job staged in shared memory
-    auto run_job = [&](int ph) {
+    // the push product and the equal-time G builder (src/dqmc_core.cpp:204-215 / :265-276):
+    // products PH_PUSH, B1, B2, the inverse, products B3, B4; each product's job is staged in
+    // shared memory (one call site of the GEMM)
+    for (int ph = 0; ph < 5; ++ph) {
+      if (ph == 3) {
+        invert_body<2>(ch, 0, true, smem, pv);
+        __syncthreads();
+        mark(6);
+      }
       if (threadIdx.x == 0) job = L[ph][c];
       __syncthreads();
       gemm_cta(job, smem, red);
-    };
-    run_job(0);
-    mark(4);
-    // ---- equal-time G builder (src/dqmc_core.cpp:204-215 / :265-276) ----
-    run_job(1);
-    run_job(2);
-    mark(5);
-    invert_body<2>(ch, 0, true, smem, pv);
-    __syncthreads();
-    mark(6);
-    run_job(3);
-    run_job(4);
+      if (ph == 0) mark(4);
+      if (ph == 2) mark(5);
+    }
     mark(7);
     if (flags & (HQ_F_MEASURE | HQ_F_SNAPSHOT)) measure_body(ch, dir, b, flags, red);
     // ---- publish: interval b of chain c is complete ----

@@ -440,10 +440,12 @@ __device__ void panel_pivot(double* A, int ld, int N, int p0, int p1, double* nr
 
 // The factorisation of the push of interval b onto stack `side` of chain `ch` (X = ch.X; U, D
 // into the stack entry b, T into W0). `smem` is the dynamic region (smem_udt_bytes); `mv` the
-// pivot moves (shared). CPW = panel columns per warp: 1 with 16 warps, 2 with 8. Every thread
+// pivot moves (shared); x_in_smem (resident only): X is already at the start of `smem` with
+// leading dimension smem_ld(N), left there by bchain_body. CPW = panel columns per warp: 1 with 16 warps, 2 with 8. Every thread
 // of the block calls it; the chain is active and b < n_stab.
 template <int CPW>
-__device__ __forceinline__ void udt_body(const HqChain& ch, int side, int b, bool resident, double* smem, PivotMoves& mv) {
+__device__ __forceinline__ void udt_body(const HqChain& ch, int side, int b, bool resident, double* smem, PivotMoves& mv,
+                                         bool x_in_smem = false) {
   const int N = ch.N;
   const int entry = b;  // push position: the pushing stack holds b entries
   const int ldp = panel_ld(N);
@@ -465,14 +467,16 @@ __device__ __forceinline__ void udt_body(const HqChain& ch, int side, int b, boo
   // formation of Q (panel i at Tc + i kQB^2)
   double* Tc = p;
   const double* X = ch.X;
-  if (resident) {
+  if (resident && x_in_smem) {
+    // X is in place already: the B chain of the same block left it at the start of smem
+  } else if (resident) {
     HQ_FOR_EACH_ELEM(N, i, j) cp_async_8(A + i + (size_t)j * ld, X + i + (size_t)j * N, true);
     cp_async_commit();
   } else {
     HQ_FOR_EACH_ELEM(N, i, j) A[i + (size_t)j * ld] = X[i + (size_t)j * N];
   }
   for (int j = threadIdx.x; j < N; j += blockDim.x) order[j] = j;
-  if (resident) cp_async_wait<0>();
+  if (resident && !x_in_smem) cp_async_wait<0>();
   __syncthreads();
   // ---- blocked Householder QR; the pivoting of the first panel is the pre-pivoting (its 16
   // columns are the first 16 of the columns sorted by decreasing norm; the order of the
