@@ -13,6 +13,13 @@ namespace hq {
 constexpr int kQB = 16;  // column panel of the blocked Householder UDV factorisation
 constexpr int kGJ = 16;  // pivot panel of the blocked Gauss-Jordan inverse
 
+// Phase hook of the factorisation bodies (invert_body, udt_body): called by every thread of the
+// block at the end of each phase with the phase's number. The kernels use this no-op; a phase
+// timer passes a hook that synchronises the block and reads the clock.
+struct NoPhase {
+  __device__ __forceinline__ void operator()(int) const {}
+};
+
 // shared-memory leading dimension of an N x N matrix: odd, so that threads walking
 // consecutive columns hit distinct banks
 __host__ __device__ constexpr inline int smem_ld(int N) { return (N % 2 == 0) ? N + 1 : N; }

@@ -140,10 +140,12 @@ __device__ void gj_panel_reg(double* A, int ld, int N, int p0, int nb, int* perm
 
 // The in-place inverse of the builder matrix `which` (0: W1, 1: W2, 2: W3, 3: W5) of chain `ch`.
 // `smem` is the dynamic region (smem_invert_bytes); pv two shared doubles. CPW = panel columns
-// per warp: 1 with 16 warps, 2 with 8. Every thread of the block calls it; the chain is active
-// and b < n_stab.
-template <int CPW>
-__device__ __forceinline__ void invert_body(const HqChain& ch, int which, bool resident, double* smem, double* pv) {
+// per warp: 1 with 16 warps, 2 with 8. Phases (phase hook): 1 panel pivots, 2 row interchanges and
+// panel staging, 3 rank update, 4 column order, 5 write-back. Every thread of the block calls it;
+// the chain is active and b < n_stab.
+template <int CPW, class Phase = NoPhase>
+__device__ __forceinline__ void invert_body(const HqChain& ch, int which, bool resident, double* smem, double* pv,
+                                            Phase phase = Phase()) {
   const int N = ch.N;
   double* src = which == 0 ? ch.W1 : (which == 1 ? ch.W2 : (which == 2 ? ch.W3 : ch.W5));
   double* A;
@@ -213,6 +215,7 @@ __device__ __forceinline__ void invert_body(const HqChain& ch, int which, bool r
       }
       __syncthreads();
     }
+    phase(1);
     // rows interchanges of this panel on every other column, then the pivot rows into Bf
     for (int j = threadIdx.x; j < N; j += blockDim.x) {
       const bool in_panel = (j >= p0 && j < p0 + nb);
@@ -231,9 +234,11 @@ __device__ __forceinline__ void invert_body(const HqChain& ch, int which, bool r
     for (int r = threadIdx.x; r < N; r += blockDim.x)
       for (int q = 0; q < nb; ++q) Wp[r + q * ldp] = A[r + (size_t)(p0 + q) * ld] - (r == p0 + q ? 1.0 : 0.0);
     __syncthreads();
+    phase(2);
     // A[:, j] += Wp Bf[:, j] for every column outside the panel (Bf is zero on the panel)
     flush_panels(A, ld, N, Wp, ldp, Bf, ldp, nb);
     __syncthreads();
+    phase(3);
   }
   // undo the row interchanges as column interchanges in reverse order: column j of the
   // inverse is column gidx[j] of A
@@ -244,6 +249,7 @@ __device__ __forceinline__ void invert_body(const HqChain& ch, int which, bool r
     }
   }
   __syncthreads();
+  phase(4);
   if (resident) {
     HQ_FOR_EACH_ELEM(N, i, j) src[i + (size_t)j * N] = A[i + (size_t)gidx[j] * ld];
   } else {
@@ -258,6 +264,7 @@ __device__ __forceinline__ void invert_body(const HqChain& ch, int which, bool r
       __syncthreads();
     }
   }
+  phase(5);
 }
 
 }  // namespace hq

@@ -441,11 +441,13 @@ __device__ void panel_pivot(double* A, int ld, int N, int p0, int p1, double* nr
 // The factorisation of the push of interval b onto stack `side` of chain `ch` (X = ch.X; U, D
 // into the stack entry b, T into W0). `smem` is the dynamic region (smem_udt_bytes); `mv` the
 // pivot moves (shared); x_in_smem (resident only): X is already at the start of `smem` with
-// leading dimension smem_ld(N), left there by bchain_body. CPW = panel columns per warp: 1 with 16 warps, 2 with 8. Every thread
-// of the block calls it; the chain is active and b < n_stab.
-template <int CPW>
+// leading dimension smem_ld(N), left there by bchain_body. CPW = panel columns per warp: 1 with 16 warps, 2 with 8. Phases
+// (phase hook): 0 load, 1 panel pivoting, 2 panel QR, 3 trailing update, 4 D and T out, 5 Q: trailing
+// blocks, 6 Q: panel columns, 7 U out. Every thread of the block calls it; the chain is active and
+// b < n_stab.
+template <int CPW, class Phase = NoPhase>
 __device__ __forceinline__ void udt_body(const HqChain& ch, int side, int b, bool resident, double* smem, PivotMoves& mv,
-                                         bool x_in_smem = false) {
+                                         bool x_in_smem = false, Phase phase = Phase()) {
   const int N = ch.N;
   const int entry = b;  // push position: the pushing stack holds b entries
   const int ldp = panel_ld(N);
@@ -478,6 +480,7 @@ __device__ __forceinline__ void udt_body(const HqChain& ch, int side, int b, boo
   for (int j = threadIdx.x; j < N; j += blockDim.x) order[j] = j;
   if (resident && !x_in_smem) cp_async_wait<0>();
   __syncthreads();
+  phase(0);
   // ---- blocked Householder QR; the pivoting of the first panel is the pre-pivoting (its 16
   // columns are the first 16 of the columns sorted by decreasing norm; the order of the
   // others does not matter, as every later panel selects by norm again) ----
@@ -485,15 +488,19 @@ __device__ __forceinline__ void udt_body(const HqChain& ch, int side, int b, boo
     const int p1 = min(p0 + kQB, N);
     if (N <= 160) {
       panel_pivot<5>(A, ld, N, p0, p1, nrm, order, rk, Vb, ldp, mv);
+      phase(1);
       qr_panel_reg<5, CPW>(A, ld, N, p0, p1, tau);
     } else {
       panel_pivot<0>(A, ld, N, p0, p1, nrm, order, rk, Vb, ldp, mv);
+      phase(1);
       qr_panel(A, ld, N, p0, p1, tau);
     }
+    phase(2);
     if (p1 < N) {
       double* Tp = Tc + (size_t)(p0 / kQB) * kQB * kQB;
       wy_forward(A, ld, N, p0, p1 - p0, tau, Vb, ldp, Tp, S, W, ldp, p1, N - p1);
     }
+    phase(3);
   }
   // ---- D = |diag R|, T = D^-1 R P^T (T[:, order[c]] = row-scaled R[:, c]) ----
   const size_t NN = (size_t)N * N;
@@ -511,6 +518,7 @@ __device__ __forceinline__ void udt_body(const HqChain& ch, int side, int b, boo
     Tout[r + (size_t)order[cc] * N] = (ir != 0.0) ? v : (r == cc ? 1.0 : 0.0);
   }
   __syncthreads();
+  phase(4);
   // ---- form Q in place, panels backwards: the trailing columns get the panel's WY
   // transformation, the panel's own columns (identity columns until now) are in closed form
   //   Q[:, p0:p1] = E - V T V[p0:p1, :]^T ----
@@ -524,6 +532,7 @@ __device__ __forceinline__ void udt_body(const HqChain& ch, int side, int b, boo
     } else {
       wy_factor(A, ld, N, p0, m, tau, Vb, ldp, T, S);
     }
+    phase(5);
     for (int t = threadIdx.x; t < kQB * kQB; t += blockDim.x) {
       const int l = t / kQB, j = t % kQB;
       double acc = 0.0;
@@ -538,9 +547,11 @@ __device__ __forceinline__ void udt_body(const HqChain& ch, int side, int b, boo
     __syncthreads();
     rank_update(A + p0 + (size_t)p0 * ld, ld, N - p0, m, Vb + p0, ldp, W, ldp, kQB);
     __syncthreads();
+    phase(6);
   }
   double* Uout = ch.stackU + ((size_t)side * ch.n_stab + entry) * NN;
   copy_mat(Uout, N, A, ld, N);
+  phase(7);
 }
 
 }  // namespace hq
