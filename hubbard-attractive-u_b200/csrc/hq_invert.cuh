@@ -64,7 +64,7 @@ __device__ __forceinline__ void gj_pivot_reg(double (&x)[RPL], int k, int N, dou
   const double vk = __shfl_sync(0xffffffffu, slot_at<RPL>(x, k), k & 31);
   const double vb = __shfl_sync(0xffffffffu, slot_at<RPL>(x, bi), bi & 31);
   const bool ok = (best > 0.0) && isfinite(best);
-  const double pinv = ok ? 1.0 / vb : 0.0;
+  const double pinv = ok ? __drcp_rn(vb) : 0.0;  // = 1 / vb, correctly rounded
 #pragma unroll
   for (int t = 0; t < RPL; ++t) {
     const int r = lane + 32 * t;
