@@ -104,7 +104,7 @@ __device__ __forceinline__ bool walk_block(const HqChain& ch, const double* G, i
     if (s < nb) {
       const int ss = s / R, si = s % R;  // g[s][*] is held by group ss at register si
       // column s, row s and the diagonal entry of the current g; gamma is formed before
-      // the decision so that its division overlaps the test
+      // the decision so that its reciprocal overlaps the test
       const double dg = __shfl_sync(0xffffffffu, r[si], ss * NB + s);
       double colr[R];
 #pragma unroll
@@ -112,7 +112,7 @@ __device__ __forceinline__ bool walk_block(const HqChain& ch, const double* G, i
       const double yv = __shfl_sync(0xffffffffu, r[si], ss * NB + c) - (c == s ? 1.0 : 0.0);
       const double dl = dls[s];
       const double av = 1.0 + (1.0 - dg) * dl;
-      const double gam = dl / av;
+      const double gam = dl * __drcp_rn(av);  // Delta / a: correctly rounded 1 / a, one product
       if (log && lane == s) myr = reference_ratio(dg, dl);
       // accept iff u < min(1, |r|), r = a^2 / (1 + Delta), 1 + Delta = e^{-2 alpha s} > 0
       const bool acc = accept_flip<EXACT>(thr[s], av, dg, dl, sh.u + b0 + s, near);
@@ -198,7 +198,7 @@ __device__ __forceinline__ bool walk_block16(const HqChain& ch, const double* G,
         rowv[b] = __shfl_sync(0xffffffffu, r[s & 3][b], 8 * (s >> 2) + cg) - (2 * cg + b == s ? 1.0 : 0.0);
       const double dl = dls[s];
       const double av = 1.0 + (1.0 - dg) * dl;
-      const double gam = dl / av;
+      const double gam = dl * __drcp_rn(av);  // Delta / a: correctly rounded 1 / a, one product
       if (log && lane == s) myr = reference_ratio(dg, dl);
       const bool acc = accept_flip<EXACT>(thr[s], av, dg, dl, sh.u + b0 + s, near);
       const double ge = acc ? gam : 0.0;
