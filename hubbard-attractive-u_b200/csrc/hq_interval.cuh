@@ -30,10 +30,15 @@ __device__ __forceinline__ void metropolis_slice_blk(const HqChain& ch, double* 
   for (int b0 = 0, bi = 0; b0 < N; b0 += NB, ++bi) {
     if (warp == 0) {
       const int nb = min(NB, N - b0);
+      // the fast walk without the ratio log unless it is on; near a tie the exact walk again
       if constexpr (NB == 16) {
-        if (walk_block16<false>(ch, G, ld, sh, b0, nb, log, bi & 1)) walk_block16<true>(ch, G, ld, sh, b0, nb, log, bi & 1);
+        const bool near = log ? walk_block16<false, true>(ch, G, ld, sh, b0, nb, true, bi & 1)
+                              : walk_block16<false, false>(ch, G, ld, sh, b0, nb, false, bi & 1);
+        if (near) walk_block16<true>(ch, G, ld, sh, b0, nb, log, bi & 1);
       } else {
-        if (walk_block<NB, false>(ch, G, ld, sh, b0, nb, log, bi & 1)) walk_block<NB, true>(ch, G, ld, sh, b0, nb, log, bi & 1);
+        const bool near = log ? walk_block<NB, false, true>(ch, G, ld, sh, b0, nb, true, bi & 1)
+                              : walk_block<NB, false, false>(ch, G, ld, sh, b0, nb, false, bi & 1);
+        if (near) walk_block<NB, true>(ch, G, ld, sh, b0, nb, log, bi & 1);
       }
     }
     __syncthreads();

@@ -196,7 +196,9 @@ __device__ __forceinline__ void cl_metropolis(const HqChain& ch, double* Gc, int
     const int owner = b0 / kNC;
     const int slot = bi & 1;
     if (rank == owner && warp == 0) {
-      if (walk_block16<false>(ch, Gs, kLd, sh, b0, 16, log, slot)) walk_block16<true>(ch, Gs, kLd, sh, b0, 16, log, slot);
+      const bool near = log ? walk_block16<false, true>(ch, Gs, kLd, sh, b0, 16, true, slot)
+                            : walk_block16<false, false>(ch, Gs, kLd, sh, b0, 16, false, slot);
+      if (near) walk_block16<true>(ch, Gs, kLd, sh, b0, 16, log, slot);
     }
     cluster.sync();  // the walk's records are visible to the cluster
     const int* o_ired = cluster.map_shared_rank(sh.ired, owner);

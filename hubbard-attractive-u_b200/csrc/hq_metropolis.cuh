@@ -67,10 +67,12 @@ __device__ __forceinline__ bool accept_flip(double thr, double av, double gii, d
 }
 
 // the walk of the block [b0, b0 + nb) by one warp (see above); writes the records and the
-// accepted count into ired[slot]; returns the near-tie flag of the fast walk
-template <int NB, bool EXACT>
+// accepted count into ired[slot]; returns the near-tie flag of the fast walk. LOGT false
+// compiles the ratio log out (log is then ignored).
+template <int NB, bool EXACT, bool LOGT = true>
 __device__ __forceinline__ bool walk_block(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0, int nb,
                            bool log, int slot) {
+  log = LOGT && log;
   constexpr int R = (NB * NB >= 32) ? NB * NB / 32 : 1;  // rows of g held by one lane
   constexpr int H = NB / R;                              // lane groups (rows h*R .. h*R+R-1)
   const int lane = threadIdx.x & 31;
@@ -103,20 +105,25 @@ __device__ __forceinline__ bool walk_block(const HqChain& ch, const double* G, i
     yk[s] = 0.0;
     if (s < nb) {
       const int ss = s / R, si = s % R;  // g[s][*] is held by group ss at register si
-      // column s, row s and the diagonal entry of the current g; gamma is formed before
-      // the decision so that its reciprocal overlaps the test
+      // column s, row s and the diagonal entry of the current g. On the step's dependency
+      // chain (g_ss -> a -> 1/a -> the rank-1 update -> the next g_ss): a as one FMA on
+      // 1 + Delta, the correctly rounded reciprocal of a (formed before the decision so that
+      // it overlaps the test), and one product with the column, which was scaled by Delta
+      // beside the chain
       const double dg = __shfl_sync(0xffffffffu, r[si], ss * NB + s);
       double colr[R];
 #pragma unroll
       for (int i = 0; i < R; ++i) colr[i] = __shfl_sync(0xffffffffu, r[i], h * NB + s);
       const double yv = __shfl_sync(0xffffffffu, r[si], ss * NB + c) - (c == s ? 1.0 : 0.0);
       const double dl = dls[s];
-      const double av = 1.0 + (1.0 - dg) * dl;
-      const double gam = dl * __drcp_rn(av);  // Delta / a: correctly rounded 1 / a, one product
-      if (log && lane == s) myr = reference_ratio(dg, dl);
+      const double av = fma(-dg, dl, 1.0 + dl);  // 1 + (1 - g_ss) Delta
+      const double rc = __drcp_rn(av);
+      const double gam = dl * rc;                // Delta / a
+      if (LOGT && log && lane == s) myr = reference_ratio(dg, dl);
       // accept iff u < min(1, |r|), r = a^2 / (1 + Delta), 1 + Delta = e^{-2 alpha s} > 0
       const bool acc = accept_flip<EXACT>(thr[s], av, dg, dl, sh.u + b0 + s, near);
       const double ge = acc ? gam : 0.0;
+      const double gr = acc ? rc : 0.0;
       double xs = colr[0];
 #pragma unroll
       for (int i = 1; i < R; ++i) xs = (c == i) ? colr[i] : xs;
@@ -124,7 +131,7 @@ __device__ __forceinline__ bool walk_block(const HqChain& ch, const double* G, i
       yk[s] = yv;
       if (lane == s) myg = gam;
 #pragma unroll
-      for (int i = 0; i < R; ++i) r[i] = fma(ge * colr[i], yv, r[i]);
+      for (int i = 0; i < R; ++i) r[i] = fma(gr * (dl * colr[i]), yv, r[i]);
       mask |= acc ? (1u << s) : 0u;
     }
   }
@@ -158,10 +165,11 @@ __device__ __forceinline__ bool walk_block(const HqChain& ch, const double* G, i
 // Every entry is updated with the same expression as in walk_block, so the two walks agree
 // bitwise. Records: lanes with cg < 4 write X[J_(4 rg + cg), m], lanes with rg < 2 write
 // Y[m, J_(2 cg + rg)].
-template <bool EXACT>
+template <bool EXACT, bool LOGT = true>
 __device__ __forceinline__ bool walk_block16(const HqChain& ch, const double* G, int ld, const MetroShared& sh, int b0,
                                              int nb, bool log, int slot) {
   constexpr int NB = 16;
+  log = LOGT && log;
   const int lane = threadIdx.x & 31;
   const int rg = lane >> 3, cg = lane & 7;
   double r[4][2];
@@ -197,11 +205,13 @@ __device__ __forceinline__ bool walk_block16(const HqChain& ch, const double* G,
       for (int b = 0; b < 2; ++b)
         rowv[b] = __shfl_sync(0xffffffffu, r[s & 3][b], 8 * (s >> 2) + cg) - (2 * cg + b == s ? 1.0 : 0.0);
       const double dl = dls[s];
-      const double av = 1.0 + (1.0 - dg) * dl;
-      const double gam = dl * __drcp_rn(av);  // Delta / a: correctly rounded 1 / a, one product
-      if (log && lane == s) myr = reference_ratio(dg, dl);
+      const double av = fma(-dg, dl, 1.0 + dl);  // 1 + (1 - g_ss) Delta (as in walk_block)
+      const double rc = __drcp_rn(av);
+      const double gam = dl * rc;                // Delta / a
+      if (LOGT && log && lane == s) myr = reference_ratio(dg, dl);
       const bool acc = accept_flip<EXACT>(thr[s], av, dg, dl, sh.u + b0 + s, near);
       const double ge = acc ? gam : 0.0;
+      const double gr = acc ? rc : 0.0;
       // the record row of this lane is 4 rg + cg (cg < 4), its record column 2 cg + rg (rg < 2)
       double xs = colr[0];
       xs = (cg == 1) ? colr[1] : xs;
@@ -212,7 +222,7 @@ __device__ __forceinline__ bool walk_block16(const HqChain& ch, const double* G,
       if (lane == s) myg = gam;
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
-        const double f = ge * colr[a];
+        const double f = gr * (dl * colr[a]);
 #pragma unroll
         for (int b = 0; b < 2; ++b) r[a][b] = fma(f, rowv[b], r[a][b]);
       }
