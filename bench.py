@@ -413,9 +413,10 @@ def run_gpu(args):
     # the timed region; its launches then occupy the GPU alone ----
     isolated = None
     if metric_wl and rank == 0 and dom_name == "interval" and not args.no_isolated:
+        ns = min(128, len(params))
         os.environ["HQ_CHAIN_GROUPS"] = "1"
         try:
-            solo = hq.Engine(params[:128], device=local)
+            solo = hq.Engine(params[:ns], device=local)
         finally:
             os.environ.pop("HQ_CHAIN_GROUPS", None)
         solo.fields_random()
@@ -435,14 +436,14 @@ def run_gpu(args):
             sd = hq.SWEEP_DOWN if sd == hq.SWEEP_UP else hq.SWEEP_UP
         a1 = solo.estimators_all()
         ic = hq.capi.PROFILE_CLASSES.index("interval")
-        ccfg = [solo.config(c) for c in range(128)]
+        ccfg = [solo.config(c) for c in range(ns)]
         fl = sum(interval_flops(p["nl"], p["nt"] * 2, a1[c, 5] - a0[c, 5], ccfg[c][1], ccfg[c][0])
-                 for c, p in enumerate(params[:128]))
+                 for c, p in enumerate(params[:ns]))
         launch_ms = ms2[ic] / max(1, cnt2[ic])
         ach = fl / max(1, cnt2[ic]) / (launch_ms * 1e-3) / 1e12
-        isolated = {"chains_per_launch": 128, "launch_ms_avg": launch_ms, "achieved": ach,
+        isolated = {"chains_per_launch": ns, "launch_ms_avg": launch_ms, "achieved": ach,
                     "frac": (ach / peak) if peak else None,
-                    "note": "k_interval timed on one stream with no other kernel beside it (a context of 128 of "
+                    "note": f"k_interval timed on one stream with no other kernel beside it (a context of {ns} of "
                             "the chains with HQ_CHAIN_GROUPS=1), outside the timed region"}
         solo.close()
     roofline["isolated"] = isolated
