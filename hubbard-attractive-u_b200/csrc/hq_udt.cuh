@@ -62,20 +62,24 @@ static __device__ void qr_panel(double* A, int ld, int N, int p0, int p1, double
 template <int RPL>
 __device__ __forceinline__ void reflector_reg(double* A, int ld, int N, int c, double (&x)[RPL], double* tau) {
   const int lane = threadIdx.x & 31;
-  double xs = 0.0, alpha = 0.0;
+  // two partial sums: the lane's part of the reflector's dependency chain is half as long
+  double xs0 = 0.0, xs1 = 0.0, alpha = 0.0;
 #pragma unroll
   for (int t = 0; t < RPL; ++t) {
     const int r = lane + 32 * t;
-    if (r > c && r < N) xs = fma(x[t], x[t], xs);
+    if (r > c && r < N) {
+      if (t & 1) xs1 = fma(x[t], x[t], xs1);
+      else xs0 = fma(x[t], x[t], xs0);
+    }
     if (r == c) alpha = x[t];
   }
-  xs = warp_sum(xs);
+  const double xs = warp_sum(xs0 + xs1);
   alpha = __shfl_sync(0xffffffffu, alpha, c & 31);
   double ti = 0.0, beta = alpha;
   if (xs > 0.0) {
     // xs is an unscaled sum of squares already, so the norm needs no hypot
     beta = -copysign(sqrt(fma(alpha, alpha, xs)), alpha);
-    ti = (beta - alpha) / beta;
+    ti = (beta - alpha) * __drcp_rn(beta);  // (beta - alpha) / beta
     const double sc = 1.0 / (alpha - beta);
 #pragma unroll
     for (int t = 0; t < RPL; ++t) {
@@ -122,14 +126,15 @@ __device__ void qr_panel_reg(double* A, int ld, int N, int p0, int p1, double* t
         const double ti = tau[c];
         if (ti != 0.0) {
           double v[RPL];
-          double w = 0.0;
+          double w0 = 0.0, w1 = 0.0;  // two partial sums (a shorter chain per lane)
 #pragma unroll
           for (int t = 0; t < RPL; ++t) {
             const int r = lane + 32 * t;
             v[t] = (r > c && r < N) ? A[r + (size_t)c * ld] : 0.0;
-            w = (r == c) ? w + x[i][t] : fma(v[t], x[i][t], w);
+            if (t & 1) w1 = (r == c) ? w1 + x[i][t] : fma(v[t], x[i][t], w1);
+            else w0 = (r == c) ? w0 + x[i][t] : fma(v[t], x[i][t], w0);
           }
-          w = warp_sum(w) * ti;
+          const double w = warp_sum(w0 + w1) * ti;
 #pragma unroll
           for (int t = 0; t < RPL; ++t) {
             const int r = lane + 32 * t;
