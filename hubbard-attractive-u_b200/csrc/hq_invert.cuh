@@ -33,6 +33,18 @@ __device__ __forceinline__ double slot_at(const double (&x)[RPL], int r) {
   return v;
 }
 
+// the same for five slots as a tree of depth 3 (bits 0, 1 and 2 of r / 32)
+template <>
+__device__ __forceinline__ double slot_at<5>(const double (&x)[5], int r) {
+  const int t = r >> 5;
+  double a, b, c, v;
+  asm("{\n\t.reg .pred p;\n\tsetp.ne.s32 p, %3, 0;\n\tselp.f64 %0, %2, %1, p;\n\t}" : "=d"(a) : "d"(x[0]), "d"(x[1]), "r"(t & 1));
+  asm("{\n\t.reg .pred p;\n\tsetp.ne.s32 p, %3, 0;\n\tselp.f64 %0, %2, %1, p;\n\t}" : "=d"(b) : "d"(x[2]), "d"(x[3]), "r"(t & 1));
+  asm("{\n\t.reg .pred p;\n\tsetp.ne.s32 p, %3, 0;\n\tselp.f64 %0, %2, %1, p;\n\t}" : "=d"(c) : "d"(a), "d"(b), "r"(t & 2));
+  asm("{\n\t.reg .pred p;\n\tsetp.ne.s32 p, %3, 0;\n\tselp.f64 %0, %2, %1, p;\n\t}" : "=d"(v) : "d"(c), "d"(x[4]), "r"(t & 4));
+  return v;
+}
+
 // pivot k of a register-resident Gauss-Jordan panel, by the warp that holds column k:
 // partial pivoting (largest |A[r][k]|, r >= k, smallest index among equals), row swap in
 // this column, the multipliers into fcol, the inverse's column k into x, and perm / pinv
@@ -40,16 +52,29 @@ template <int RPL>
 __device__ __forceinline__ void gj_pivot_reg(double (&x)[RPL], int k, int N, double* fcol, double* pinv_out,
                                              int* perm, double* status) {
   const int lane = threadIdx.x & 31;
-  double best = -1.0;
-  int bi = N;
+  // the lane's candidate: the largest |x[t]| over its rows r >= k, the smallest such row among
+  // equals; rows out of range and NaNs are (-1, N) and never win. A pairwise tree over the slots
+  // (depth 3 for five) gives the same pair as a scan in row order.
+  double cv[RPL];
+  int cr[RPL];
 #pragma unroll
   for (int t = 0; t < RPL; ++t) {
     const int r = lane + 32 * t;
-    if (r >= k && r < N) {
-      const double v = fabs(x[t]);
-      if (v > best || (v == best && r < bi)) { best = v; bi = r; }
-    }
+    const double v = fabs(x[t]);
+    const bool ok = r >= k && r < N && v == v;
+    cv[t] = ok ? v : -1.0;
+    cr[t] = ok ? r : N;
   }
+#pragma unroll
+  for (int w = 1; w < RPL; w *= 2)
+#pragma unroll
+    for (int t = 0; t + w < RPL; t += 2 * w) {
+      const bool tb = cv[t + w] > cv[t] || (cv[t + w] == cv[t] && cr[t + w] < cr[t]);
+      cv[t] = tb ? cv[t + w] : cv[t];
+      cr[t] = tb ? cr[t + w] : cr[t];
+    }
+  double best = cv[0];
+  int bi = cr[0];
   // warp argmax with three redux steps on the bit pattern of |x| (monotonic for non-negative
   // doubles; NaNs were skipped by the lane-local search): the high word, then the low word
   // among the lanes holding the maximum, then the smallest row among those
